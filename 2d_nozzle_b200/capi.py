@@ -1,0 +1,147 @@
+"""ctypes binding of ``include/nozzle_b200.h``.
+
+The library is loaded from the package's ``_lib`` directory (built by
+:mod:`.build`).  A missing or unloadable library raises immediately: there is
+no CPU fallback anywhere in this package.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libnozzle_b200.so")
+
+P = C.c_void_p
+I64 = C.c_int64
+I32 = C.c_int32
+
+
+class Mesh(C.Structure):
+    _fields_ = [
+        ("kind", I32),
+        ("order", I32),
+        ("affine", I32),
+        ("reserved", I32),
+        ("n_elem", I64),
+        ("n_edge", I64),
+        ("geo", P),
+        ("gx", P),
+        ("gy", P),
+        ("minv", P),
+        ("mean_w", P),
+        ("area", P),
+        ("face_nbr", P),
+        ("face_code", P),
+        ("face_edge", P),
+        ("edge_geo", P),
+    ]
+
+
+class Physics(C.Structure):
+    _fields_ = [
+        ("gamma", C.c_double),
+        ("entropy_fix", C.c_double),
+        ("hllc_low_mach", C.c_double),
+        ("flux", I32),
+        ("limiter", I32),
+        ("in_cos", C.c_double),
+        ("in_sin", C.c_double),
+        ("in_at2", C.c_double),
+        ("in_at", C.c_double),
+        ("in_rho_t", C.c_double),
+        ("p_back", C.c_double),
+        ("bf_rho_t", C.c_double),
+        ("bf_p_t", C.c_double),
+        ("bf_band", C.c_double),
+        ("lim_fraction", C.c_double),
+        ("rho_floor", C.c_double),
+        ("p_floor", C.c_double),
+        ("lebesgue", C.c_double),
+        ("lim_steps", I32),
+        ("reserved", I32),
+        ("norm_w", C.c_double * 4),
+    ]
+
+
+class StageArgs(C.Structure):
+    _fields_ = [
+        ("V", P),
+        ("U0", P),
+        ("out", P),
+        ("dt", P),
+        ("norm_partial", P),
+        ("counters", P),
+        ("flags", P),
+        ("dt_factor", C.c_double),
+        ("a", C.c_double),
+        ("b", C.c_double),
+        ("stage", I32),
+        ("reserved", I32),
+    ]
+
+
+class Buffers(C.Structure):
+    _fields_ = [
+        ("S0", P),
+        ("S1", P),
+        ("S2", P),
+        ("dt", P),
+        ("norm_partial", P),
+        ("res", P),
+        ("counters", P),
+    ]
+
+
+# (name, restype, argtypes) of every exported symbol
+SIGNATURES = [
+    ("nzb_version", C.c_int, []),
+    ("nzb_last_error", C.c_char_p, []),
+    ("nzb_table_size", I64, [C.c_int, C.c_int]),
+    ("nzb_upload_tables", C.c_int, [C.c_int, C.c_int, P, I64]),
+    ("nzb_pack_state", C.c_int, [P, P, I64, C.c_int, P, P]),
+    ("nzb_unpack_state", C.c_int, [P, P, I64, C.c_int, P, P]),
+    ("nzb_residual", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.c_int, P, P, P, P]),
+    ("nzb_inverse_mass", C.c_int, [C.POINTER(Mesh), P, P, P]),
+    ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
+    ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
+    ("nzb_norm_blocks", I64, [I64]),
+    ("nzb_element_blocks", I64, [C.POINTER(Mesh)]),
+    ("nzb_norm_finalize", C.c_int, [P, I64, C.c_double, P, P]),
+    ("nzb_norm", C.c_int, [P, I64, C.c_int, P, P, P, P]),
+    ("nzb_solver_create", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(Buffers), C.c_int, C.c_double, C.POINTER(P)]),
+    ("nzb_solver_run", C.c_int, [P, C.c_int, P]),
+    ("nzb_solver_destroy", C.c_int, [P]),
+]
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def load(path: str = LIB_PATH):
+    """Load the library once and declare every signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise NativeError(
+            f"{path} is missing; build it with `python 2d_nozzle_b200/build.py` (nvcc, sm_100a). "
+            "This backend has no CPU fallback."
+        )
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = _lib.nzb_last_error().decode(errors="replace") if _lib is not None else "library not loaded"
+        raise NativeError(f"{what} failed ({rc}): {msg}")

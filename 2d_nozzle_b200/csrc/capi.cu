@@ -1,0 +1,466 @@
+// capi.cu -- the C ABI: table upload, kernel dispatch, layout conversion,
+// norms, and the graph-captured steady-march solver.
+//
+// Dispatch instantiates the element kernel for triangles p = 0..3 (affine and
+// general geometry) and quadrilaterals p = 0..3 (general geometry).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <set>
+#include <string>
+#include <utility>
+
+#include "element.cuh"
+#include "nozzle_b200.h"
+
+namespace nzb {
+
+static thread_local std::string g_err;
+
+static int fail(const std::string& msg) {
+  g_err = msg;
+  return -1;
+}
+
+static int cuda_check(cudaError_t st, const char* what) {
+  if (st != cudaSuccess) return fail(std::string(what) + ": " + cudaGetErrorString(st));
+  return 0;
+}
+
+static int launch_check(const char* what) { return cuda_check(cudaGetLastError(), what); }
+
+static std::mutex g_tab_mu;
+static std::set<std::pair<int, int>> g_tab_done;  // (device, kind * 16 + order)
+
+static bool tables_ready(int kind, int order) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  return g_tab_done.count({dev, kind * 16 + order}) != 0;
+}
+
+static int check_mesh(const nzb_mesh* m) {
+  if (!m) return fail("mesh is null");
+  if (m->kind != NZB_TRI && m->kind != NZB_QUAD) return fail("unknown element kind");
+  if (m->order < 0 || m->order > MAX_ORDER) return fail("order must lie in 0..3");
+  if (m->affine && m->kind != NZB_TRI) return fail("affine geometry is for straight-sided triangles");
+  if (m->n_elem <= 0) return fail("mesh has no elements");
+  if (!m->area || !m->face_nbr || !m->face_code || !m->face_edge || !m->edge_geo)
+    return fail("mesh arrays area/face_nbr/face_code/face_edge/edge_geo are required");
+  if (m->affine ? !m->geo : (!m->gx || !m->gy || !m->minv || !m->mean_w))
+    return fail(m->affine ? "affine mesh needs geo" : "general mesh needs gx, gy, minv, mean_w");
+  if (!tables_ready(m->kind, m->order)) return fail("reference tables not uploaded for this kind/order on this device");
+  return 0;
+}
+
+constexpr int NT = 128;  // threads per block of the helper kernels
+
+// Element-kernel blocks for (kind, order): 128 threads, or 64 for cubic quads.
+static int block_threads(int kind, int order) {
+  switch (kind * 16 + order) {
+#define NZB_BT(K, P) \
+  case K * 16 + P: return Launch<K, P>::NT;
+    NZB_BT(0, 0) NZB_BT(0, 1) NZB_BT(0, 2) NZB_BT(0, 3) NZB_BT(1, 0) NZB_BT(1, 1) NZB_BT(1, 2) NZB_BT(1, 3)
+#undef NZB_BT
+  }
+  return 128;
+}
+
+static int64_t blocks_for(int64_t n) { return (n + NT - 1) / NT; }
+static int64_t element_blocks(const nzb_mesh& m) {
+  const int bt = block_threads(m.kind, m.order);
+  return (m.n_elem + bt - 1) / bt;
+}
+
+template <int K, int P, bool AFF>
+static int launch_element(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
+  const int64_t nb = element_blocks(m);
+  if (nb > 0x7fffffff) return fail("too many elements for one launch");
+  k_element<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  return launch_check("element kernel launch");
+}
+
+static int dispatch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
+#define NZB_CASE(K, P)                                                                \
+  if (m.kind == K && m.order == P) {                                                  \
+    if (K == 0 && m.affine) return launch_element<K, P, (K == 0)>(m, ph, w, st);      \
+    return launch_element<K, P, false>(m, ph, w, st);                                 \
+  }
+  NZB_CASE(0, 0)
+  NZB_CASE(0, 1)
+  NZB_CASE(0, 2)
+  NZB_CASE(0, 3)
+  NZB_CASE(1, 0)
+  NZB_CASE(1, 1)
+  NZB_CASE(1, 2)
+  NZB_CASE(1, 3)
+#undef NZB_CASE
+  return fail("unsupported kind/order");
+}
+
+// ---- layout conversion ------------------------------------------------------
+__global__ void k_pack(const double* __restrict__ src, double* __restrict__ dst, int64_t E, int np,
+                       const int32_t* __restrict__ perm) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * np) return;
+  const int64_t e = t % E;
+  const int i = (int)(t / E);
+  const int64_t r = perm ? perm[e] : e;
+  const double* p = src + (r * np + i) * 4;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) dst[((int64_t)s * np + i) * E + e] = p[s];
+}
+
+__global__ void k_unpack(const double* __restrict__ src, double* __restrict__ dst, int64_t E, int np,
+                         const int32_t* __restrict__ perm) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * np) return;
+  const int64_t e = t % E;
+  const int i = (int)(t / E);
+  const int64_t r = perm ? perm[e] : e;
+  double* p = dst + (r * np + i) * 4;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) p[s] = src[((int64_t)s * np + i) * E + e];
+}
+
+// ---- norms --------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_norm_partial(const double* __restrict__ A, int64_t E, int np,
+                                                     double w0, double w1, double w2, double w3,
+                                                     double* __restrict__ partial) {
+  const int64_t e = (int64_t)blockIdx.x * NT + threadIdx.x;
+  double acc = 0.0;
+  if (e < E) {
+    const double w[4] = {w0, w1, w2, w3};
+    for (int s = 0; s < 4; ++s)
+      for (int i = 0; i < np; ++i) {
+        const double v = A[((int64_t)s * np + i) * E + e] * w[s];
+        acc = fma(v, v, acc);
+      }
+  }
+  block_sum_store<NT / 32>(acc, partial + blockIdx.x);
+}
+
+// One block, fixed order: thread t sums slots t, t + 1024, ...; then a tree.
+__global__ void __launch_bounds__(1024) k_norm_finalize(const double* __restrict__ partial, int64_t n,
+                                                        double count, double* __restrict__ out) {
+  __shared__ double red[1024];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += 1024) acc += partial[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sqrt(red[0] / count);
+}
+
+__global__ void k_inverse_mass_general(const double* __restrict__ minv, const double* __restrict__ R,
+                                       double* __restrict__ out, int64_t E, int np) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  for (int s = 0; s < 4; ++s)
+    for (int i = 0; i < np; ++i) {
+      double acc = 0.0;
+      for (int j = 0; j < np; ++j)
+        acc = fma(minv[((int64_t)i * np + j) * E + e], R[((int64_t)s * np + j) * E + e], acc);
+      out[((int64_t)s * np + i) * E + e] = acc;
+    }
+}
+
+template <int K, int P>
+__global__ void k_inverse_mass_affine(const double* __restrict__ geo, const double* __restrict__ R,
+                                      double* __restrict__ out, int64_t E) {
+  using S = Shape<K, P>;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const double det = geo[4 * E + e];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double r[S::NP];
+#pragma unroll
+    for (int j = 0; j < S::NP; ++j) r[j] = R[((int64_t)s * S::NP + j) * E + e];
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < S::NP; ++j) acc = fma(tab<K, P>(S::O_MINV + i * S::NP + j), r[j], acc);
+      out[((int64_t)s * S::NP + i) * E + e] = acc / det;
+    }
+  }
+}
+
+// ---- solver ---------------------------------------------------------------------
+struct Solver {
+  nzb_mesh mesh;
+  nzb_physics phys;
+  nzb_buffers buf;
+  int ssprk3;
+  double dt_factor;
+  int device;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;
+};
+
+static int enqueue_step(const Solver& s, cudaStream_t st) {
+  Work w{};
+  w.op = OP_STAGE;
+  w.dt = s.buf.dt;
+  w.counters = s.buf.counters;
+  w.dt_factor = s.dt_factor;
+  // stage 1: S0 -> S2 (ssprk3) or S0 -> S1 (euler), with dt and the norm
+  w.V = s.buf.S0;
+  w.U0 = nullptr;
+  w.out = s.ssprk3 ? s.buf.S2 : s.buf.S1;
+  w.norm_partial = s.buf.norm_partial;
+  w.stage = 1;
+  w.a = 0.0;
+  w.b = 1.0;
+  if (dispatch(s.mesh, s.phys, w, st)) return -1;
+  if (!s.ssprk3) {
+    return cuda_check(cudaMemcpyAsync(s.buf.S0, s.buf.S1, sizeof(double) * 4 * s.mesh.n_elem *
+                                                              n_basis(s.mesh.kind, s.mesh.order),
+                                      cudaMemcpyDeviceToDevice, st),
+                      "euler copy-back");
+  }
+  w.norm_partial = nullptr;
+  // stage 2: S1 = limit(3/4 S0 + 1/4 (S2 + dt F(S2)))
+  w.V = s.buf.S2;
+  w.U0 = s.buf.S0;
+  w.out = s.buf.S1;
+  w.stage = 2;
+  w.a = 0.75;
+  w.b = 0.25;
+  if (dispatch(s.mesh, s.phys, w, st)) return -1;
+  // stage 3: S0 = limit(1/3 S0 + 2/3 (S1 + dt F(S1))), in place over U0
+  w.V = s.buf.S1;
+  w.U0 = s.buf.S0;
+  w.out = s.buf.S0;
+  w.stage = 3;
+  w.a = 1.0 / 3.0;
+  w.b = 2.0 / 3.0;
+  return dispatch(s.mesh, s.phys, w, st);
+}
+
+static int graph_for(Solver& s, int n, cudaGraphExec_t* out) {
+  auto it = s.graphs.find(n);
+  if (it != s.graphs.end()) {
+    *out = it->second;
+    return 0;
+  }
+  cudaGraph_t g = nullptr;
+  if (cuda_check(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return -1;
+  int rc = 0;
+  for (int i = 0; i < n && rc == 0; ++i) rc = enqueue_step(s, s.stream);
+  const cudaError_t end = cudaStreamEndCapture(s.stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return -1;
+  }
+  if (cuda_check(end, "end capture")) return -1;
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t inst = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (cuda_check(inst, "graph instantiate")) return -1;
+  s.graphs[n] = ex;
+  *out = ex;
+  return 0;
+}
+
+}  // namespace nzb
+
+using namespace nzb;
+
+extern "C" {
+
+int nzb_version(void) { return 1; }
+
+const char* nzb_last_error(void) { return g_err.c_str(); }
+
+int64_t nzb_table_size(int kind, int order) {
+  if ((kind != 0 && kind != 1) || order < 0 || order > MAX_ORDER) return -1;
+  return slot_size(kind, order);
+}
+
+int nzb_upload_tables(int kind, int order, const double* tables, int64_t n) {
+  if (nzb_table_size(kind, order) < 0) return fail("unsupported kind/order");
+  if (n != slot_size(kind, order)) return fail("table size mismatch");
+  if (!tables) return fail("tables is null");
+  if (cuda_check(cudaMemcpyToSymbol(c_tab, tables, sizeof(double) * n, sizeof(double) * slot_offset(kind, order)),
+                 "table upload"))
+    return -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tab_mu);
+  g_tab_done.insert({dev, kind * 16 + order});
+  return 0;
+}
+
+int nzb_pack_state(const double* src, double* dst, int64_t E, int np, const int32_t* perm, void* stream) {
+  if (!src || !dst || E <= 0 || np <= 0) return fail("pack: bad arguments");
+  const int64_t n = E * np;
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(src, dst, E, np, perm);
+  return launch_check("pack launch");
+}
+
+int nzb_unpack_state(const double* src, double* dst, int64_t E, int np, const int32_t* perm, void* stream) {
+  if (!src || !dst || E <= 0 || np <= 0) return fail("unpack: bad arguments");
+  const int64_t n = E * np;
+  k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(src, dst, E, np, perm);
+  return launch_check("unpack launch");
+}
+
+int nzb_residual(const nzb_mesh* mesh, const nzb_physics* phys, int op, const double* U, double* out,
+                 double* wave, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !U || !out) return fail("residual: null argument");
+  if (op != NZB_OP_RESIDUAL && op != NZB_OP_RATE) return fail("residual: unknown op");
+  if (U == out) return fail("residual: out must not alias U");
+  Work w{};
+  w.op = op == NZB_OP_RESIDUAL ? OP_RESIDUAL : OP_RATE;
+  w.V = U;
+  w.out = out;
+  w.wave = wave;
+  return dispatch(*mesh, *phys, w, (cudaStream_t)stream);
+}
+
+int nzb_inverse_mass(const nzb_mesh* mesh, const double* R, double* out, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!R || !out) return fail("inverse_mass: null argument");
+  const int64_t E = mesh->n_elem;
+  const unsigned nb = (unsigned)((E + 127) / 128);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!mesh->affine) {
+    k_inverse_mass_general<<<nb, 128, 0, st>>>(mesh->minv, R, out, E, n_basis(mesh->kind, mesh->order));
+    return launch_check("inverse mass launch");
+  }
+  switch (mesh->order) {
+    case 0: k_inverse_mass_affine<0, 0><<<nb, 128, 0, st>>>(mesh->geo, R, out, E); break;
+    case 1: k_inverse_mass_affine<0, 1><<<nb, 128, 0, st>>>(mesh->geo, R, out, E); break;
+    case 2: k_inverse_mass_affine<0, 2><<<nb, 128, 0, st>>>(mesh->geo, R, out, E); break;
+    default: k_inverse_mass_affine<0, 3><<<nb, 128, 0, st>>>(mesh->geo, R, out, E); break;
+  }
+  return launch_check("inverse mass launch");
+}
+
+int nzb_limit(const nzb_mesh* mesh, const nzb_physics* phys, double* U, unsigned long long* counters,
+              uint8_t* flags, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !U) return fail("limit: null argument");
+  Work w{};
+  w.op = OP_LIMIT;
+  w.V = U;
+  w.out = U;
+  w.counters = counters;
+  w.flags = flags;
+  return dispatch(*mesh, *phys, w, (cudaStream_t)stream);
+}
+
+int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_args* a, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !a || !a->V || !a->out || !a->dt) return fail("stage: null argument");
+  if (a->stage < 1 || a->stage > 3) return fail("stage must be 1, 2 or 3");
+  if (a->stage > 1 && !a->U0) return fail("stages 2 and 3 need U0");
+  if (a->out == a->V) return fail("stage: out must not alias V");
+  Work w{};
+  w.op = OP_STAGE;
+  w.V = a->V;
+  w.U0 = a->U0;
+  w.out = a->out;
+  w.dt = a->dt;
+  w.norm_partial = a->norm_partial;
+  w.counters = a->counters;
+  w.flags = a->flags;
+  w.dt_factor = a->dt_factor;
+  w.a = a->a;
+  w.b = a->b;
+  w.stage = a->stage;
+  return dispatch(*mesh, *phys, w, (cudaStream_t)stream);
+}
+
+int64_t nzb_norm_blocks(int64_t n_elem) { return n_elem <= 0 ? 0 : (n_elem + 63) / 64; }
+
+int64_t nzb_element_blocks(const nzb_mesh* mesh) { return mesh ? element_blocks(*mesh) : -1; }
+
+int nzb_norm_finalize(const double* partial, int64_t n_partial, double count, double* out, void* stream) {
+  if (!partial || !out || n_partial <= 0 || !(count > 0)) return fail("norm_finalize: bad arguments");
+  k_norm_finalize<<<1, 1024, 0, (cudaStream_t)stream>>>(partial, n_partial, count, out);
+  return launch_check("norm finalize launch");
+}
+
+int nzb_norm(const double* A, int64_t E, int np, const double* w4, double* partial, double* out, void* stream) {
+  if (!A || !w4 || !partial || !out || E <= 0 || np <= 0) return fail("norm: bad arguments");
+  const int64_t nb = blocks_for(E);
+  k_norm_partial<<<(unsigned)nb, NT, 0, (cudaStream_t)stream>>>(A, E, np, w4[0], w4[1], w4[2], w4[3], partial);
+  if (launch_check("norm launch")) return -1;
+  return nzb_norm_finalize(partial, nb, 4.0 * (double)E * np, out, stream);
+}
+
+int nzb_solver_create(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_buffers* buf, int scheme_ssprk3,
+                      double dt_factor, nzb_solver** out) {
+  if (!out) return fail("solver_create: out is null");
+  *out = nullptr;
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !buf || !buf->S0 || !buf->S1 || !buf->dt || !buf->norm_partial || !buf->res || !buf->counters)
+    return fail("solver_create: missing buffer");
+  if (scheme_ssprk3 && !buf->S2) return fail("solver_create: ssprk3 needs S2");
+  Solver* s = new Solver();
+  s->mesh = *mesh;
+  s->phys = *phys;
+  s->buf = *buf;
+  s->ssprk3 = scheme_ssprk3 ? 1 : 0;
+  s->dt_factor = dt_factor;
+  cudaGetDevice(&s->device);
+  if (cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "solver stream") ||
+      cuda_check(cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming), "solver event") ||
+      cuda_check(cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming), "solver event")) {
+    nzb_solver_destroy(reinterpret_cast<nzb_solver*>(s));
+    return -1;
+  }
+  *out = reinterpret_cast<nzb_solver*>(s);
+  return 0;
+}
+
+int nzb_solver_run(nzb_solver* solver, int n_steps, void* stream) {
+  Solver* s = reinterpret_cast<Solver*>(solver);
+  if (!s) return fail("solver is null");
+  if (n_steps < 1) return fail("n_steps must be at least 1");
+  cudaStream_t caller = (cudaStream_t)stream;
+  if (cuda_check(cudaEventRecord(s->ev_in, caller), "event record") ||
+      cuda_check(cudaStreamWaitEvent(s->stream, s->ev_in, 0), "stream wait"))
+    return -1;
+  // chunks of up to 64 steps share one captured graph per size
+  int left = n_steps;
+  while (left > 0) {
+    const int n = left > 64 ? 64 : left;
+    cudaGraphExec_t ex = nullptr;
+    if (graph_for(*s, n, &ex)) return -1;
+    if (cuda_check(cudaGraphLaunch(ex, s->stream), "graph launch")) return -1;
+    left -= n;
+  }
+  const int np = n_basis(s->mesh.kind, s->mesh.order);
+  if (nzb_norm_finalize(s->buf.norm_partial, element_blocks(s->mesh), 4.0 * (double)s->mesh.n_elem * np,
+                        s->buf.res, s->stream))
+    return -1;
+  if (cuda_check(cudaEventRecord(s->ev_out, s->stream), "event record") ||
+      cuda_check(cudaStreamWaitEvent(caller, s->ev_out, 0), "stream wait"))
+    return -1;
+  return 0;
+}
+
+int nzb_solver_destroy(nzb_solver* solver) {
+  Solver* s = reinterpret_cast<Solver*>(solver);
+  if (!s) return 0;
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  if (s->ev_in) cudaEventDestroy(s->ev_in);
+  if (s->ev_out) cudaEventDestroy(s->ev_out);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,456 @@
+// element.cuh -- the fused element kernel: volume term, face fluxes, lift,
+// inverse mass, stage update and positivity limiter in one pass per element.
+//
+// One thread owns one element.  Its NP x 4 coefficients and NP x 4 residual
+// accumulators live in registers; every reference-element table is read from
+// constant memory at a compile-time address, so each multiply-add is a single
+// DFMA with a constant-bank operand.  The face integral is computed from the
+// element's own side: both traces are formed (the neighbour's from the p + 1
+// coefficients on the shared edge, read straight from HBM/L2), and the flux is
+// evaluated with the owner's trace as the left state and the owner's normal, so
+// the owner and the neighbour of an edge compute bit-identical fluxes and the
+// scheme stays conservative with no edge array and no second pass.
+//
+// Mathematics (src/spatial/assembly.py:52-162, src/backends/_numba_kernels.py:
+// 484-777): R_i = -sum_q (gx_iq F_q + gy_iq G_q) + sum_f sign_f sum_q phi_f,iq fw_q
+// with fw = flux * |dX/dsigma| * w_q, the rate -M^-1 R, and
+// wave = sum_f max_q s_q * length_f.  For straight-sided triangles
+// gx = det * w_q (dphi/dxi xi_x + dphi/deta eta_x) and M = det * M_ref, so the
+// kernel carries five numbers per element instead of the reference's
+// per-element operator arrays.
+#pragma once
+#include "physics.cuh"
+#include "shapes.cuh"
+
+namespace nzb {
+
+__constant__ double c_tab[TABLE_DOUBLES];
+
+
+enum { OP_RESIDUAL = 0, OP_RATE = 1, OP_STAGE = 2, OP_LIMIT = 3 };
+
+struct Work {
+  int op;
+  const double* V;   // state the rate is evaluated at
+  const double* U0;  // step start state (stages 2 and 3)
+  double* out;
+  double* wave;
+  double* dt;
+  double* norm_partial;
+  unsigned long long* counters;
+  uint8_t* flags;
+  double dt_factor, a, b;
+  int stage;
+};
+
+template <int K, int P>
+__device__ __forceinline__ double tab(int idx) {
+  return c_tab[idx];
+}
+
+// Minimum density and pressure over the limiter's probe set -- volume points
+// plus the element's own face points -- of ubar + theta (u - ubar).  With raw
+// set the probe values are used as they are, as the reference's violation test
+// does (src/spatial/limiter.py:224-228); otherwise through the scaling formula
+// (src/spatial/limiter.py:146-148,151-178).
+template <int K, int P>
+__device__ __forceinline__ void probe_minima(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4],
+                                             double theta, bool raw, double g, double& rmin, double& pmin) {
+  using S = Shape<K, P>;
+  rmin = 1e300;
+  pmin = 1e300;
+  auto visit = [&](double w0, double w1, double w2, double w3) {
+    if (!raw) {
+      w0 = ub[0] + theta * (w0 - ub[0]);
+      w1 = ub[1] + theta * (w1 - ub[1]);
+      w2 = ub[2] + theta * (w2 - ub[2]);
+      w3 = ub[3] + theta * (w3 - ub[3]);
+    }
+    rmin = w0 < rmin ? w0 : rmin;
+    const double r = w0 < 1e-300 ? 1e-300 : w0;
+    const double pp = (g - 1.0) * (w3 - 0.5 * (w1 * w1 + w2 * w2) / r);
+    pmin = pp < pmin ? pp : pmin;
+  };
+#pragma unroll
+  for (int q = 0; q < S::NQV; ++q) {
+    double w[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i) {
+      const double phi = tab<K, P>(S::O_PHI + i * S::NQV + q);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w[s] = fma(phi, u[i][s], w[s]);
+    }
+    visit(w[0], w[1], w[2], w[3]);
+  }
+#pragma unroll
+  for (int f = 0; f < S::NF; ++f) {
+#pragma unroll
+    for (int q = 0; q < S::NQF; ++q) {
+      double w[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int j = 0; j < S::NE; ++j) {
+        const double l = tab<K, P>(S::O_E1D + j * S::NQF + q);
+        const int n = edge_node(K, P, f, j);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) w[s] = fma(l, u[n][s], w[s]);
+      }
+      visit(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+// Zhang-Shu positivity limiter of one element, in place
+// (src/spatial/limiter.py:103-243; the O(NP) Lebesgue screen of
+// src/backends/_numba_kernels.py:1010-1026 skips provably admissible elements).
+template <int K, int P, bool AFF>
+__device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], const nzb_mesh& m,
+                                              const nzb_physics& ph, int64_t e, int& scaled, int& repaired) {
+  using S = Shape<K, P>;
+  const double g = ph.gamma;
+  const int64_t E = m.n_elem;
+  double mw[S::NP];
+#pragma unroll
+  for (int i = 0; i < S::NP; ++i) mw[i] = AFF ? tab<K, P>(S::O_MW + i) : __ldg(m.mean_w + i * E + e);
+  double ub[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < S::NP; ++i)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u[i][s], ub[s]);
+
+  // last-resort repair of a non-physical cell average
+  const double rho_new = ub[0] < ph.rho_floor ? ph.rho_floor : ub[0];
+  const double e_min = ph.p_floor / (g - 1.0) + 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / rho_new;
+  const double rhoE_new = ub[3] < e_min ? e_min : ub[3];
+  if (ub[0] < ph.rho_floor || ub[3] < e_min) {
+    const double d0 = rho_new - ub[0], d3 = rhoE_new - ub[3];
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i) {
+      u[i][0] += d0;
+      u[i][3] += d3;
+    }
+    repaired = 1;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) ub[s] = 0.0;
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u[i][s], ub[s]);
+  }
+  const double pbar = (g - 1.0) * (ub[3] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / ub[0]);
+  double eps_r = ph.lim_fraction * ub[0];
+  eps_r = eps_r < 0.5 * ph.rho_floor ? 0.5 * ph.rho_floor : eps_r;
+  double eps_p = ph.lim_fraction * pbar;
+  eps_p = eps_p < 0.5 * ph.p_floor ? 0.5 * ph.p_floor : eps_p;
+
+  // sufficient screen: bound every probe through the Lebesgue constant
+  double dev[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < S::NP; ++i)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) dev[s] = fmax(dev[s], fabs(u[i][s] - ub[s]));
+  const double lam = ph.lebesgue;
+  const double rho_lo = ub[0] - lam * dev[0];
+  if (rho_lo >= eps_r) {
+    const double m_hi = sqrt(ub[1] * ub[1] + ub[2] * ub[2]) + lam * sqrt(dev[1] * dev[1] + dev[2] * dev[2]);
+    const double p_lo = (g - 1.0) * (ub[3] - lam * dev[3] - 0.5 * m_hi * m_hi / rho_lo);
+    if (p_lo >= eps_p) return;
+  }
+  double rmin, pmin;
+  probe_minima<K, P>(u, ub, 1.0, true, g, rmin, pmin);
+  if (!(rmin < eps_r) && !(pmin < eps_p)) return;
+
+  double theta = 1.0;
+  if (rmin < eps_r) {
+    const double gap = ub[0] - rmin;
+    theta = (ub[0] - eps_r) / (gap > 0.0 ? gap : 1.0);
+    theta = theta < 0.0 ? 0.0 : (theta > 1.0 ? 1.0 : theta);
+  }
+  double r_unused, p_hi;
+  probe_minima<K, P>(u, ub, theta, false, g, r_unused, p_hi);
+  if (!(p_hi >= eps_p)) {
+    double lo = 0.0, hi = theta;
+    for (int it = 0; it < ph.lim_steps; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      double pm;
+      probe_minima<K, P>(u, ub, mid, false, g, r_unused, pm);
+      if (pm >= eps_p)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    theta = lo;
+  }
+#pragma unroll
+  for (int i = 0; i < S::NP; ++i)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) u[i][s] = ub[s] + theta * (u[i][s] - ub[s]);
+  scaled = 1;
+}
+
+template <int NW>
+__device__ __forceinline__ void block_sum_store(double v, double* dst) {
+  __shared__ double red[NW];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) t += red[w];
+    *dst = t;
+  }
+}
+
+// Threads per block: 128, or 64 where the per-thread face accumulator would
+// push static shared memory past 48 KB (cubic quadrilaterals).
+template <int K, int P>
+struct Launch {
+  static constexpr int NP = Shape<K, P>::NP;
+  static constexpr int NT = (NP * 4 * 8 * 128 <= 40 * 1024) ? 128 : 64;
+};
+
+template <int K, int P, bool AFF>
+__global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, const nzb_physics ph, const Work w) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
+  constexpr int BT = Launch<K, P>::NT;
+  // face contributions, one column per thread: facc[(i * 4 + s) * BT + t]
+  __shared__ double facc[NP * 4 * BT];
+  const int t = threadIdx.x;
+  const int64_t E = m.n_elem;
+  const int64_t e = (int64_t)blockIdx.x * BT + t;
+  const bool active = e < E;
+  const double g = ph.gamma;
+  double nrm = 0.0;
+  int scaled = 0, repaired = 0;
+
+  if (active && w.op == OP_LIMIT) {
+    double u[NP][4];
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) u[i][s] = w.V[(s * NP + i) * E + e];
+    if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = u[i][s];
+    if (w.flags) w.flags[e] = (uint8_t)(scaled | (repaired << 1));
+  } else if (active) {
+    const bool rate = w.op != OP_RESIDUAL;
+    double xx = 0, xy = 0, yx = 0, yy = 0, det = 1.0;
+    if (AFF) {
+      xx = __ldg(m.geo + 0 * E + e);
+      xy = __ldg(m.geo + 1 * E + e);
+      yx = __ldg(m.geo + 2 * E + e);
+      yy = __ldg(m.geo + 3 * E + e);
+      det = __ldg(m.geo + 4 * E + e);
+    }
+#pragma unroll
+    for (int i = 0; i < NP * 4; ++i) facc[i * BT + t] = 0.0;
+
+    // ---- face terms: a rolled loop over (face, point), so the flux code is
+    // inlined once.  The element's own and its neighbour's edge coefficients
+    // are read from HBM/L2; the lift goes to the shared-memory column.
+    const double fs = (AFF && rate) ? -1.0 / det : 1.0;
+    double wave = 0.0;
+#pragma unroll 1
+    for (int f = 0; f < NF; ++f) {
+      const int code = __ldg(m.face_code + f * E + e);
+      const int k = __ldg(m.face_edge + f * E + e);
+      const int nb = __ldg(m.face_nbr + f * E + e);
+      const bool side = code & 1;
+      const int nf = (code >> 1) & 7;
+      const int tag = code >> 4;
+      const double nx = __ldg(m.edge_geo + 4 * (int64_t)k + 0);
+      const double ny = __ldg(m.edge_geo + 4 * (int64_t)k + 1);
+      const double jac = __ldg(m.edge_geo + 4 * (int64_t)k + 2);
+      const double len = __ldg(m.edge_geo + 4 * (int64_t)k + 3);
+      double ue[NE][4], un[NE][4];
+      int node[NE];
+#pragma unroll
+      for (int j = 0; j < NE; ++j) {
+        node[j] = edge_node(K, P, f, j);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) ue[j][s] = __ldg(w.V + (s * NP + node[j]) * E + e);
+      }
+      if (nb >= 0) {
+        // the neighbour's edge coefficients in the edge's (owner's) orientation
+#pragma unroll
+        for (int j = 0; j < NE; ++j) {
+          const int n = edge_node(K, P, nf, side ? j : NE - 1 - j);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) un[j][s] = __ldg(w.V + (s * NP + n) * E + nb);
+        }
+      }
+      const double coef = (side ? -1.0 : 1.0) * fs;
+      double smax = 0.0;
+#pragma unroll 1
+      for (int q = 0; q < NQF; ++q) {
+        // side 1 walks the edge backwards: l_j(1 - sigma_q) = l_{p-j}(sigma_q)
+        double cj[NE], lj[NE];
+#pragma unroll
+        for (int j = 0; j < NE; ++j) {
+          lj[j] = c_tab[S::O_E1D + j * NQF + q];
+          const double r = c_tab[S::O_E1D + (NE - 1 - j) * NQF + q];
+          cj[j] = side ? r : lj[j];
+        }
+        double tc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < NE; ++j)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) tc[s] = fma(cj[j], ue[j][s], tc[s]);
+        double F[4], sp;
+        if (nb >= 0) {
+          double tn[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int j = 0; j < NE; ++j)
+#pragma unroll
+            for (int s = 0; s < 4; ++s) tn[s] = fma(lj[j], un[j][s], tn[s]);
+          double L[4], R[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            L[s] = side ? tn[s] : tc[s];
+            R[s] = side ? tc[s] : tn[s];
+          }
+          sp = interface_flux(L, R, nx, ny, ph, F);
+        } else {
+          sp = boundary_flux(tag, tc, nx, ny, ph, F);
+        }
+        smax = sp > smax ? sp : smax;
+        const double scale = jac * c_tab[S::O_WF + q];
+        double fwc[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) fwc[s] = (F[s] * scale) * coef;
+#pragma unroll
+        for (int j = 0; j < NE; ++j)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            double& a = facc[(node[j] * 4 + s) * BT + t];
+            a = fma(cj[j], fwc[s], a);
+          }
+      }
+      wave += smax * len;
+    }
+    if (w.wave) w.wave[e] = wave;
+
+    // ---- volume term, fully unrolled, tables as constant-bank operands
+    double acc[NP][4];
+    {
+      double u[NP][4];
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          u[i][s] = __ldg(w.V + (s * NP + i) * E + e);
+          acc[i][s] = facc[(i * 4 + s) * BT + t];
+        }
+      const double vs = (AFF && !rate) ? -det : 1.0;
+#pragma unroll
+      for (int q = 0; q < NQV; ++q) {
+        double uq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          const double phi = tab<K, P>(S::O_PHI + i * NQV + q);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) uq[s] = fma(phi, u[i][s], uq[s]);
+        }
+        const Prim pr = primitives(uq, g);
+        const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
+        const double G[4] = {pr.rho * pr.vy, pr.rho * pr.vx * pr.vy, pr.rho * pr.vy * pr.vy + pr.p, pr.rho * pr.vy * pr.H};
+        if (AFF) {
+          double fx[4], fe[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            fx[s] = (xx * F[s] + xy * G[s]) * vs;
+            fe[s] = (yx * F[s] + yy * G[s]) * vs;
+          }
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double a = tab<K, P>(S::O_WXI + i * NQV + q);
+            const double b = tab<K, P>(S::O_WETA + i * NQV + q);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) acc[i][s] = fma(a, fx[s], fma(b, fe[s], acc[i][s]));
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double gx = __ldg(m.gx + (i * NQV + q) * E + e);
+            const double gy = __ldg(m.gy + (i * NQV + q) * E + e);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) acc[i][s] -= gx * F[s] + gy * G[s];
+          }
+        }
+      }
+    }
+
+    if (w.op == OP_RESIDUAL) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = acc[i][s];
+    } else {
+      double dt = 0.0;
+      if (w.op == OP_STAGE) {
+        if (w.stage == 1) {
+          const double d = wave < FLOOR ? FLOOR : wave;
+          dt = w.dt_factor * 2.0 * __ldg(m.area + e) / d;
+          w.dt[e] = dt;
+        } else {
+          dt = w.dt[e];
+        }
+      }
+      // rate = -M^-1 R, consumed row by row; the stage update overwrites u
+      double u[NP][4];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          double r = 0.0;
+          if (AFF) {
+#pragma unroll
+            for (int j = 0; j < NP; ++j) r = fma(tab<K, P>(S::O_MINV + i * NP + j), acc[j][s], r);
+          } else {
+#pragma unroll
+            for (int j = 0; j < NP; ++j) r = fma(__ldg(m.minv + (i * NP + j) * E + e), acc[j][s], r);
+            r = -r;
+          }
+          if (w.op == OP_RATE) {
+            w.out[(s * NP + i) * E + e] = r;
+          } else {
+            const double v = __ldg(w.V + (s * NP + i) * E + e);
+            if (w.stage == 1) {
+              const double rw = r * ph.norm_w[s];
+              nrm = fma(rw, rw, nrm);
+              u[i][s] = v + dt * r;
+            } else {
+              const double u0 = __ldg(w.U0 + (s * NP + i) * E + e);
+              u[i][s] = w.a * u0 + w.b * (v + dt * r);
+            }
+          }
+        }
+      }
+      if (w.op == OP_STAGE) {
+        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = u[i][s];
+        if (w.flags) w.flags[e] = (uint8_t)(scaled | (repaired << 1));
+      }
+    }
+  }
+  // block-level reductions (every thread of the block reaches these)
+  if (w.op == OP_STAGE && w.norm_partial && w.stage == 1) block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
+  if ((w.op == OP_STAGE || w.op == OP_LIMIT) && w.counters) {
+    const int ns = __syncthreads_count(scaled);
+    const int nr = __syncthreads_count(repaired);
+    if (t == 0) {
+      if (ns) atomicAdd(w.counters + 0, (unsigned long long)ns);
+      if (nr) atomicAdd(w.counters + 1, (unsigned long long)nr);
+    }
+  }
+}
+
+}  // namespace nzb

@@ -1,0 +1,188 @@
+/*
+ * nozzle_b200.h -- C ABI of the B200 nodal-DG backend for the 2D Euler nozzle.
+ *
+ * Every entry point takes plain pointers and sizes.  Device arrays are owned
+ * by the caller (the Python backend allocates them as torch tensors); the
+ * library never allocates, frees or retains device memory except inside a
+ * solver object, which only records the caller's pointers.  Every function
+ * returns 0 on success and a negative code on failure, with a message from
+ * nzb_last_error().  Numerical failure (NaN, overflow) is not an error: it
+ * propagates into the returned residual, as in the reference solver.
+ *
+ * Device layouts ("SoA"): a state is (4, NP, E) doubles -- component s, node i,
+ * element e at [(s * NP + i) * E + e] -- so a warp reading one (s, i) plane
+ * reads 32 consecutive elements.  The reference's (E, NP, 4) layout is
+ * converted by nzb_pack_state / nzb_unpack_state.
+ *
+ * Reference interfaces replaced (reference repository paths):
+ *   nzb_residual (op RESIDUAL)   Backend.residual          src/backends/base.py:118-120,
+ *                                 assembly.residual         src/spatial/assembly.py:153-157
+ *   nzb_residual (op RATE)       NumbaBackend._rate_into    src/backends/numba_backend.py:213-234,
+ *                                 _numba_kernels.element_rate src/backends/_numba_kernels.py:586-664
+ *   nzb_inverse_mass             Backend.inverse_mass      src/backends/base.py:122-124
+ *   nzb_limit                    Backend.limit / positivity_limit
+ *                                 src/backends/numba_backend.py:247-281,
+ *                                 src/backends/_numba_kernels.py:927-1093
+ *   nzb_stage                    stage / combine_ssp / local_dt / rms_weighted fused
+ *                                 src/backends/_numba_kernels.py:789-850
+ *   nzb_norm                     Backend.norm              src/backends/numba_backend.py:178-181
+ *   nzb_solver_*                 NumbaBackend.run          src/backends/numba_backend.py:283-337
+ */
+#ifndef NOZZLE_B200_H
+#define NOZZLE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Element kinds and the flux / boundary codes used in the arrays below. */
+enum { NZB_TRI = 0, NZB_QUAD = 1 };
+enum { NZB_ROE = 0, NZB_HLLC = 1, NZB_AUSMUP = 2 };
+enum { NZB_INFLOW = 1, NZB_OUTFLOW = 2, NZB_WALL = 3, NZB_AXIS = 4 };
+enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
+
+/* Mesh and operators of one mesh, all device pointers, all owned by the caller.
+ *
+ * affine = 1: straight-sided triangles; geo holds (5, E) = xi_x, xi_y, eta_x,
+ *             eta_y, det and the volume / mass operators come from the
+ *             reference-element tables uploaded by nzb_upload_tables.
+ * affine = 0: any element; gx, gy hold (NP*NQV, E) weighted gradients
+ *             w det dphi/dx (the reference's Operators.grad_x / grad_y),
+ *             minv (NP*NP, E) the inverse mass matrices, mean_w (NP, E).
+ * face_nbr  (NF, E): element across face f, or -1 on a boundary.
+ * face_code (NF, E): side (bit 0: 0 owner, 1 neighbour) | neighbour's local
+ *             face << 1 | boundary tag << 4.
+ * face_edge (NF, E): global edge id.
+ * edge_geo  (n_edge, 4): nx, ny (owner's outward unit normal), |dX/dsigma|,
+ *             edge length.  Edges are straight: one normal per edge.
+ */
+typedef struct {
+  int32_t kind;
+  int32_t order;
+  int32_t affine;
+  int32_t reserved;
+  int64_t n_elem;
+  int64_t n_edge;
+  const double* geo;
+  const double* gx;
+  const double* gy;
+  const double* minv;
+  const double* mean_w;
+  const double* area;
+  const int32_t* face_nbr;
+  const int32_t* face_code;
+  const int32_t* face_edge;
+  const double* edge_geo;
+} nzb_mesh;
+
+/* Gas, operating point and limiter constants, evaluated on the host exactly
+ * as the reference evaluates them (src/config.py, src/physics/boundary.py). */
+typedef struct {
+  double gamma;
+  double entropy_fix;
+  double hllc_low_mach;
+  int32_t flux;
+  int32_t limiter;        /* 0 none, 1 positivity (ignored at p = 0) */
+  /* inflow: cos/sin of the inflow angle, a_t^2 = gamma R T_t, a_t, rho_t */
+  double in_cos, in_sin, in_at2, in_at, in_rho_t;
+  /* outflow: back pressure, backflow reservoir density (0 = off), p_t, band */
+  double p_back, bf_rho_t, bf_p_t, bf_band;
+  /* positivity limiter */
+  double lim_fraction, rho_floor, p_floor, lebesgue;
+  int32_t lim_steps;
+  int32_t reserved;
+  /* residual-norm component weights (1, 1/a_t, 1/a_t, 1/a_t^2) */
+  double norm_w[4];
+} nzb_physics;
+
+/* Tables of one reference element: see the packer in layout.py for the order.
+ * Must be called once per device and (kind, order) before any other call on
+ * that kind and order.  Host pointer. */
+int nzb_upload_tables(int kind, int order, const double* tables, int64_t n);
+/* Number of doubles nzb_upload_tables expects for (kind, order). */
+int64_t nzb_table_size(int kind, int order);
+
+/* Reference (E, NP, 4) <-> device (4, NP, E).  perm (nullable) maps device
+ * element index -> reference element index. */
+int nzb_pack_state(const double* src_aos, double* dst_soa, int64_t n_elem, int np,
+                   const int32_t* perm, void* stream);
+int nzb_unpack_state(const double* src_soa, double* dst_aos, int64_t n_elem, int np,
+                     const int32_t* perm, void* stream);
+
+/* op RESIDUAL: out = R(U) with M dU/dt = -R.  op RATE: out = -M^-1 R(U).
+ * wave (nullable) receives sum_f s_f l_f per element. */
+int nzb_residual(const nzb_mesh* mesh, const nzb_physics* phys, int op, const double* U,
+                 double* out, double* wave, void* stream);
+
+/* out = M^-1 R. */
+int nzb_inverse_mass(const nzb_mesh* mesh, const double* R, double* out, void* stream);
+
+/* Positivity limiter in place.  counters (nullable, device, 2 x uint64)
+ * accumulate (scaled, repaired); flags (nullable, device, E bytes) receive
+ * bit 0 = scaled, bit 1 = cell mean repaired. */
+int nzb_limit(const nzb_mesh* mesh, const nzb_physics* phys, double* U,
+              unsigned long long* counters, uint8_t* flags, void* stream);
+
+/* One fused explicit stage:
+ *   stage 1: dt_e = dt_factor * 2 A_e / max(wave_e, 1e-10) (written to dt),
+ *            out = limit(V + dt F(V)),  norm_partial[block] = sum (w F)^2
+ *   stage 2: out = limit(a U0 + b (V + dt F(V)))   (dt read)
+ * out may alias U0 (each element reads only its own U0) but not V.
+ * norm_partial, counters, flags are nullable.  norm_partial needs
+ * nzb_norm_blocks(E) doubles. */
+typedef struct {
+  const double* V;
+  const double* U0;
+  double* out;
+  double* dt;
+  double* norm_partial;
+  unsigned long long* counters;
+  uint8_t* flags;
+  double dt_factor;
+  double a;
+  double b;
+  int32_t stage;
+  int32_t reserved;
+} nzb_stage_args;
+int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_args* args, void* stream);
+
+/* Upper bound on the partial-sum slots any kernel here writes for n_elem
+ * elements (size norm_partial buffers with it). */
+int64_t nzb_norm_blocks(int64_t n_elem);
+/* Blocks (= partial-sum slots written by stage 1) of the element kernel. */
+int64_t nzb_element_blocks(const nzb_mesh* mesh);
+/* out[0] = sqrt(sum partial[0..n_partial) / count) -- fixed summation order. */
+int nzb_norm_finalize(const double* partial, int64_t n_partial, double count, double* out, void* stream);
+/* Weighted RMS of a (4, NP, E) array: out[0] = sqrt(mean((w_s A)^2)).
+ * partial needs nzb_norm_blocks(E) doubles of scratch. */
+int nzb_norm(const double* A, int64_t n_elem, int np, const double* w4, double* partial, double* out,
+             void* stream);
+
+/* A steady-march solver over caller-owned buffers.  Every step maps S0 -> S0
+ * (scratch S1, S2); a chunk of n steps is captured once as a CUDA graph and
+ * replayed.  res (device double) receives the norm of the last step's stage-1
+ * rate; counters (device 2 x uint64) accumulate limiter activity. */
+typedef struct nzb_solver nzb_solver;
+typedef struct {
+  double* S0;
+  double* S1;
+  double* S2;
+  double* dt;
+  double* norm_partial;
+  double* res;
+  unsigned long long* counters;
+} nzb_buffers;
+int nzb_solver_create(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_buffers* buf,
+                      int scheme_ssprk3, double dt_factor, nzb_solver** out);
+int nzb_solver_run(nzb_solver* solver, int n_steps, void* stream);
+int nzb_solver_destroy(nzb_solver* solver);
+
+const char* nzb_last_error(void);
+int nzb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NOZZLE_B200_H */

@@ -1,0 +1,249 @@
+"""Generate the golden fixtures in this directory from the reference solver.
+
+Run from the repository root with the reference importable as ``src``::
+
+    PYTHONPATH=<reference checkout> python tests/golden/make_golden.py
+
+Every array here comes from the reference's own code path (its NumPy backend
+for per-stage values, its Numba backend for the long converged solve); nothing
+is computed by this repository.  The fixtures pin both the CPU oracle and the
+host-side mesh/operator builder, and the GPU tests compare against them.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {name}: {os.path.getsize(path) / 1024:.0f} KiB")
+
+
+def ref_violates(U, ops, flow, fraction=1e-8):
+    """The set of elements the reference's positivity limiter scales.
+
+    Evaluated with the reference's own limiter helpers, in the order
+    ``positivity_limiter`` uses them (src/spatial/limiter.py:216-228).  The
+    limiter's output cannot be used for this: it rebuilds every element as
+    ``ubar + theta (U - ubar)``, which moves unlimited ones by round-off.
+    """
+    from src.spatial import limiter as lim
+
+    g = flow.gamma
+    rho_floor, p_floor = lim.reference_floors(flow, fraction)
+    U = lim.floor_cell_means(U, ops, flow, fraction=fraction)
+    ubar = lim.cell_means(U, ops)
+    probes = lim.probe_values(U, ops)
+    p_bar = (g - 1.0) * (ubar[..., 3] - 0.5 * (ubar[..., 1] ** 2 + ubar[..., 2] ** 2) / ubar[..., 0])
+    eps_rho = np.maximum(fraction * ubar[..., 0], 0.5 * rho_floor)
+    eps_p = np.maximum(fraction * p_bar, 0.5 * p_floor)
+    return (probes[..., 0].min(axis=1) < eps_rho) | (lim._pressure_at(probes, g, np).min(axis=1) < eps_p)
+
+
+def _stage_record(bk, U, scheme):
+    """One step of the reference base-class stepper, recording each stage."""
+    F0, wave = bk.rate(U)
+    dt = bk.time_step(wave)
+    res = bk.norm(F0)
+    stages = []
+
+    def lim(V):
+        stages.append(ref_violates(V, bk.ops, bk.flow))
+        return bk.limit(V)
+
+    if scheme == "euler":
+        return lim(U + dt * F0), res, stages, wave, F0
+    U1 = lim(U + dt * F0)
+    F1, _ = bk.rate(U1)
+    U2 = lim(0.75 * U + 0.25 * (U1 + dt * F1))
+    F2, _ = bk.rate(U2)
+    U3 = lim((1.0 / 3.0) * U + (2.0 / 3.0) * (U2 + dt * F2))
+    return U3, res, stages, wave, F0
+
+
+def random_state(n_elem, nbf, seed=0):
+    rng = np.random.default_rng(seed)
+    base = np.array([2.0, 0.6, 0.02, 5.0])
+    return np.ascontiguousarray(base * (1.0 + 0.03 * rng.standard_normal((n_elem, nbf, 4))))
+
+
+def microbench_state(n_elem, nbf, gamma=1.4, seed=0):
+    """Per-node density lognormal(0,0.3), Mach U[0.2,3], random angle, p lognormal(0,0.5)."""
+    rng = np.random.default_rng(seed)
+    shape = (n_elem, nbf)
+    rho = rng.lognormal(0.0, 0.3, shape)
+    mach = rng.uniform(0.2, 3.0, shape)
+    ang = rng.uniform(0.0, 2.0 * np.pi, shape)
+    p = rng.lognormal(0.0, 0.5, shape)
+    a = np.sqrt(gamma * p / rho)
+    vx, vy = mach * a * np.cos(ang), mach * a * np.sin(ang)
+    E = p / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy)
+    return np.ascontiguousarray(np.stack([rho, rho * vx, rho * vy, E], -1))
+
+
+def operator_arrays(cs):
+    ops = cs.operators
+    ed = cs.topology.edges
+    return dict(
+        node_coords=np.asarray(cs.node_coords),
+        elem_nodes=cs.topology.elem_nodes,
+        face_edge=ed.face_edge,
+        face_side=ed.face_side,
+        iedge_elem=ed.iedge_elem,
+        bedge_tag=ed.bedge_tag,
+        grad_x_m=np.asarray(ops.grad_x_m),
+        grad_y_m=np.asarray(ops.grad_y_m),
+        face_basis_m=np.asarray(ops.face_basis_m),
+        inv_mass=np.asarray(ops.inv_mass),
+        edge_normal=np.asarray(ops.edge_normal),
+        edge_jac=np.asarray(ops.edge_jac),
+        edge_length=np.asarray(ops.edge_length),
+        elem_area=np.asarray(ops.elem_area),
+        mean_weights=np.asarray(ops.mean_weights),
+    )
+
+
+def per_flux(cs, U, fluxes=("roe", "hllc", "ausmup"), **flow_kw):
+    from src.backends import get_backend
+    from src.config import SolverOptions
+
+    out = {}
+    for name in fluxes:
+        flow = cs.flow.replace(flux=name, **flow_kw)
+        bk = get_backend("numpy", cs.operators, flow, SolverOptions(limiter="positivity"))
+        R, wave = bk.residual(U)
+        out[f"R_{name}"] = np.asarray(R)
+        out[f"wave_{name}"] = np.asarray(wave)
+        out[f"rate_{name}"] = -np.asarray(bk.inverse_mass(R))
+    return out
+
+
+def small_cases():
+    from src.api import build_case
+    from src.backends import get_backend
+    from src.config import SolverOptions
+    from src.spatial import limiter as lim
+
+    for kind, orders in (("tri", (0, 1, 2, 3)), ("quad", (1, 2, 3))):
+        for p in orders:
+            cs = build_case(contour="smooth", element=kind, order=p, refine=0)
+            ops = cs.operators
+            U = random_state(ops.n_elem, ops.ref.n_basis)
+            arrays = operator_arrays(cs)
+            arrays["U"] = U
+            arrays.update(per_flux(cs, U))
+            arrays.update({k + "_backflow": v for k, v in per_flux(cs, U, ("roe",), backflow=True).items()})
+            # a state with violations, for the limiter
+            Ubad = U.copy()
+            if p > 0:
+                Ubad[3, 0, 0] = -0.5
+                Ubad[7, 1, 3] = -1.0
+                Ubad[11, :, 0] = -5.0
+            arrays["U_bad"] = Ubad
+            arrays["limited_bad"] = lim.positivity_limiter(Ubad, ops, cs.flow)
+            # three steps of each scheme from the random state
+            for scheme in ("euler", "ssprk3"):
+                bk = get_backend("numpy", ops, cs.flow, SolverOptions(limiter="positivity", scheme=scheme))
+                V, res = bk.run(U.copy(), 3, scheme)
+                arrays[f"run3_{scheme}"] = np.asarray(V)
+                arrays[f"run3_{scheme}_res"] = np.float64(res)
+            _save(f"tiny_{kind}_p{p}.npz", **arrays)
+
+
+def rectangle_microbench():
+    """Config-2 distribution at 20x10 cells, cubic triangles, unit rectangle."""
+    from src.backends import get_backend
+    from src.config import FlowConditions, SolverOptions
+    from src.geometry.mesh import structured_nozzle_topology
+    from src.spatial.operators import build_operators
+
+    topo, xf, rf = structured_nozzle_topology("tri", nx=20, nr=10)
+    X, Y = np.meshgrid(xf, rf)
+    coords = np.column_stack([X.ravel(), Y.ravel()])
+    ops = build_operators(topo, coords, 3)
+    U = microbench_state(ops.n_elem, ops.ref.n_basis)
+    arrays = {"node_coords": coords, "U": U}
+    for name in ("roe", "hllc", "ausmup"):
+        flow = FlowConditions(flux=name)
+        bk = get_backend("numpy", ops, flow, SolverOptions(limiter="positivity", cfl=0.5))
+        R, wave = bk.residual(U)
+        arrays[f"R_{name}"] = np.asarray(R)
+        arrays[f"wave_{name}"] = np.asarray(wave)
+        U3, res, stages, _, _ = _stage_record(bk, U.copy(), "ssprk3")
+        arrays[f"step_{name}"] = U3
+        arrays[f"step_{name}_res"] = np.float64(res)
+        arrays[f"step_{name}_limited"] = np.stack(stages)
+    _save("rect_tri_p3.npz", **arrays)
+
+
+def config1():
+    """Smooth contour, AR 2.5, p=1 triangles, refine 1, Roe, cfl 0.5, tol 1e-10."""
+    from src.api import build_case, solve_nozzle
+    from src.post.postprocess import performance
+    from src.timestepping import initialize as ini
+
+    kw = dict(contour="smooth", area_ratio=2.5, element="tri", order=1, refine=1, flux="roe", back_pressure_ratio=0.15)
+    cs = build_case(**kw)
+    U0 = ini.initial_state(cs.operators, cs.flow, cs.geometry, "quasi1d")
+    res = solve_nozzle(case=cs, cfl=0.5, tolerance=1e-10, limiter="positivity", scheme="ssprk3", backend="numba", verbose=False)
+    perf = performance(res)
+    it, hist = res.history.as_arrays()
+    _save(
+        "config1.npz",
+        node_coords=np.asarray(cs.node_coords),
+        U0=np.asarray(U0),
+        U_final=np.asarray(res.U),
+        converged=np.bool_(res.converged),
+        iterations=np.int64(res.iterations),
+        residual=np.float64(res.residual),
+        residual_scale=np.float64(res.residual_scale),
+        history_iterations=it,
+        history_residual=hist,
+        thrust=np.float64(perf.thrust),
+        mass_flow_in=np.float64(perf.mass_flow_in),
+        exit_mach=np.float64(perf.exit_mach_area_averaged),
+        throat_height=np.float64(cs.geometry.throat_height()),
+        length=np.float64(cs.geometry.length),
+    )
+
+
+def config3(n_steps=5):
+    """Conical AR 3.0, p=3 quads, refine 3, HLLC, pb 0.6: fixed-step record."""
+    from src.api import build_case
+    from src.backends import get_backend
+    from src.config import SolverOptions
+    from src.timestepping import initialize as ini
+
+    cs = build_case(contour="conical", area_ratio=3.0, element="quad", order=3, refine=3, flux="hllc",
+                    back_pressure_ratio=0.6, allow_shock_in_nozzle=True)
+    U0 = np.asarray(ini.initial_state(cs.operators, cs.flow, cs.geometry, "quasi1d"))
+    bk = get_backend("numpy", cs.operators, cs.flow, SolverOptions(limiter="positivity", scheme="ssprk3"))
+    U = U0.copy()
+    ress, masks = [], []
+    for _ in range(n_steps):
+        U, res, stages, _, _ = _stage_record(bk, U, "ssprk3")
+        ress.append(res)
+        masks.extend(stages)
+    _save("config3.npz", node_coords=np.asarray(cs.node_coords), U0=U0, U_final=U, res=np.asarray(ress),
+          limited=np.stack(masks), n_steps=np.int64(n_steps))
+
+
+if __name__ == "__main__":
+    import src  # noqa: F401  -- fails loudly when the reference is not on PYTHONPATH
+
+    which = sys.argv[1:] or ["small", "rect", "config1", "config3"]
+    if "small" in which:
+        small_cases()
+    if "rect" in which:
+        rectangle_microbench()
+    if "config1" in which:
+        config1()
+    if "config3" in which:
+        config3()
