@@ -184,6 +184,42 @@ class B200Backend:
             return self.ssprk3_step
         raise ValueError(f"unknown scheme {scheme!r}; choose from {SCHEMES}")
 
+    def step_record(self, U, scheme: str | None = None):
+        """One step through the fused stage kernels, stage by stage.
+
+        Returns ``(U_new, residual, flags)`` with ``flags`` of shape
+        ``(stages, E)``: bit 0 = the limiter scaled the element at that stage,
+        bit 1 = its cell mean was repaired.  Same kernels as :meth:`run`.
+        """
+        torch = self.torch
+        scheme = scheme or self.scheme
+        S0, S1, S2 = self._S
+        self.mesh.pack(U, S0)
+        E = self.mesh.E
+        n_st = 3 if scheme == "ssprk3" else 1
+        flags = torch.zeros((n_st, E), dtype=torch.uint8, device=self.mesh.device)
+        factor = self.positivity_scale() * step_coefficient(self.ops.ref.order, self.opts.cfl, self.scheme)
+        plan = [(S0, None, S2 if n_st == 3 else S1, 1, 0.0, 1.0)]
+        if n_st == 3:
+            plan += [(S2, S0, S1, 2, 0.75, 0.25), (S1, S0, S0, 3, 1.0 / 3.0, 2.0 / 3.0)]
+        for k, (V, U0, out, stage, a, b) in enumerate(plan):
+            args = capi.StageArgs()
+            args.V, args.out, args.dt = V.data_ptr(), out.data_ptr(), self._dt.data_ptr()
+            args.U0 = U0.data_ptr() if U0 is not None else None
+            args.norm_partial = self._partial.data_ptr() if stage == 1 else None
+            args.counters = self._counters.data_ptr()
+            args.flags = flags[k].data_ptr()
+            args.dt_factor, args.a, args.b, args.stage = factor, a, b, stage
+            capi.check(self.lib.nzb_stage(self.mesh.c_ref, self._phys_ref, capi.C.byref(args), self._stream), "nzb_stage")
+            if stage == 1:
+                nb = int(self.lib.nzb_element_blocks(self.mesh.c_ref))
+                capi.check(self.lib.nzb_norm_finalize(self._partial.data_ptr(), nb, 4.0 * E * self.mesh.np_,
+                                                      self._res.data_ptr(), self._stream), "nzb_norm_finalize")
+        final = S0 if n_st == 3 else S1
+        out = self._host(self.mesh.unpack(final))
+        self._take_counters(n_st)
+        return out, float(self._host(self._res)[0]), self._host(flags)
+
     # -- the fused march -------------------------------------------------------
     def _solver(self, scheme: str) -> int:
         if scheme in self._solvers:

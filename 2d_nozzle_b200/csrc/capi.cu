@@ -58,7 +58,9 @@ static int check_mesh(const nzb_mesh* m) {
 
 constexpr int NT = 128;  // threads per block of the helper kernels
 
-// Element-kernel blocks for (kind, order): 128 threads, or 64 for cubic quads.
+static int64_t blocks_for(int64_t n) { return (n + NT - 1) / NT; }
+// Element-kernel blocks for (kind, order): one thread per element, 128 per
+// block, or 64 for cubic quads.
 static int block_threads(int kind, int order) {
   switch (kind * 16 + order) {
 #define NZB_BT(K, P) \
@@ -68,8 +70,6 @@ static int block_threads(int kind, int order) {
   }
   return 128;
 }
-
-static int64_t blocks_for(int64_t n) { return (n + NT - 1) / NT; }
 static int64_t element_blocks(const nzb_mesh& m) {
   const int bt = block_threads(m.kind, m.order);
   return (m.n_elem + bt - 1) / bt;
@@ -79,7 +79,10 @@ template <int K, int P, bool AFF>
 static int launch_element(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
   const int64_t nb = element_blocks(m);
   if (nb > 0x7fffffff) return fail("too many elements for one launch");
-  k_element<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  if (w.op == OP_STAGE || w.op == OP_LIMIT)
+    k_element<K, P, AFF, true><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  else
+    k_element<K, P, AFF, false><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
   return launch_check("element kernel launch");
 }
 

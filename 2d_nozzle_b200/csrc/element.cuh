@@ -48,54 +48,100 @@ __device__ __forceinline__ double tab(int idx) {
   return c_tab[idx];
 }
 
-// Minimum density and pressure over the limiter's probe set -- volume points
-// plus the element's own face points -- of ubar + theta (u - ubar).  With raw
-// set the probe values are used as they are, as the reference's violation test
-// does (src/spatial/limiter.py:224-228); otherwise through the scaling formula
-// (src/spatial/limiter.py:146-148,151-178).
+// One probe point (volume point pt < NQV, else own face point) of this
+// element's solution: w = sum_i basis_i(pt) u_i.  pt is the same on every lane
+// of the warp (the loops over points are rolled and uniform), so the table
+// reads are constant-cache broadcasts and the kernel stays small.
 template <int K, int P>
-__device__ __forceinline__ void probe_minima(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4],
-                                             double theta, bool raw, double g, double& rmin, double& pmin) {
+__device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4], int pt, double (&w)[4]) {
   using S = Shape<K, P>;
-  rmin = 1e300;
-  pmin = 1e300;
-  auto visit = [&](double w0, double w1, double w2, double w3) {
-    if (!raw) {
-      w0 = ub[0] + theta * (w0 - ub[0]);
-      w1 = ub[1] + theta * (w1 - ub[1]);
-      w2 = ub[2] + theta * (w2 - ub[2]);
-      w3 = ub[3] + theta * (w3 - ub[3]);
-    }
-    rmin = w0 < rmin ? w0 : rmin;
-    const double r = w0 < 1e-300 ? 1e-300 : w0;
-    const double pp = (g - 1.0) * (w3 - 0.5 * (w1 * w1 + w2 * w2) / r);
-    pmin = pp < pmin ? pp : pmin;
-  };
-#pragma unroll
-  for (int q = 0; q < S::NQV; ++q) {
-    double w[4] = {0.0, 0.0, 0.0, 0.0};
+  w[0] = w[1] = w[2] = w[3] = 0.0;
+  if (pt < S::NQV) {
 #pragma unroll
     for (int i = 0; i < S::NP; ++i) {
-      const double phi = tab<K, P>(S::O_PHI + i * S::NQV + q);
+      const double phi = c_tab[S::O_PHI + i * S::NQV + pt];
 #pragma unroll
       for (int s = 0; s < 4; ++s) w[s] = fma(phi, u[i][s], w[s]);
     }
-    visit(w[0], w[1], w[2], w[3]);
-  }
+  } else {
+    const int f = (pt - S::NQV) / S::NQF, q = (pt - S::NQV) - f * S::NQF;
 #pragma unroll
-  for (int f = 0; f < S::NF; ++f) {
+    for (int j = 0; j < S::NE; ++j) {
+      const double l = c_tab[S::O_E1D + j * S::NQF + q];
+      const int n = edge_node(K, P, f, j);
+      // u is indexed at a runtime node: select it from the unrolled candidates
+      double v[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
 #pragma unroll
-    for (int q = 0; q < S::NQF; ++q) {
-      double w[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int ff = 0; ff < S::NF; ++ff) {
+        const int nn = edge_node(K, P, ff, j);
+        if (ff == f) {
 #pragma unroll
-      for (int j = 0; j < S::NE; ++j) {
-        const double l = tab<K, P>(S::O_E1D + j * S::NQF + q);
-        const int n = edge_node(K, P, f, j);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) w[s] = fma(l, u[n][s], w[s]);
+          for (int s = 0; s < 4; ++s) v[s] = u[nn][s];
+        }
       }
-      visit(w[0], w[1], w[2], w[3]);
+      (void)n;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w[s] = fma(l, v[s], w[s]);
     }
+  }
+}
+
+__device__ __forceinline__ double pressure_at(const double (&w)[4], double g) {
+  const double r = w[0] < 1e-300 ? 1e-300 : w[0];
+  return (g - 1.0) * (w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / r);
+}
+
+// Minimum density and pressure over the limiter's probe set -- volume points
+// plus the element's own face points -- of ubar + theta (u - ubar), through the
+// reference's scaling formula (src/spatial/limiter.py:146-148,151-178).
+template <int K, int P>
+__device__ __forceinline__ double pmin_at(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4], double theta,
+                                          double g) {
+  double pmin = 1e300;
+#pragma unroll 1
+  for (int pt = 0; pt < Shape<K, P>::NPROBE; ++pt) {
+    double w[4];
+    probe_point<K, P>(u, pt, w);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) w[s] = ub[s] + theta * (w[s] - ub[s]);
+    const double pp = pressure_at(w, g);
+    pmin = pp < pmin ? pp : pmin;
+  }
+  return pmin;
+}
+
+// One pass over the probe points: the raw minima the reference's violation
+// test uses (src/spatial/limiter.py:224-228), and t*, the smallest positive t
+// at which p(ubar + t (w - ubar)) = eps_p at some point w.  Along the segment
+// h(t) = rho(t) (p(t) - eps_p) / (gamma - 1) = a t^2 + b t + c with
+// h(0) = rho_bar (p_bar - eps_p) / (gamma - 1) > 0; t* = 1e300 when no point binds.
+template <int K, int P>
+__device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4],
+                                           double eps_p, double g, double& rmin, double& pmin, double& tstar) {
+  const double e1 = eps_p / (g - 1.0);
+  const double c = ub[3] * ub[0] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) - e1 * ub[0];
+  rmin = 1e300;
+  pmin = 1e300;
+  tstar = 1e300;
+#pragma unroll 1
+  for (int pt = 0; pt < Shape<K, P>::NPROBE; ++pt) {
+    double w[4];
+    probe_point<K, P>(u, pt, w);
+    rmin = w[0] < rmin ? w[0] : rmin;
+    const double pp = pressure_at(w, g);
+    pmin = pp < pmin ? pp : pmin;
+    const double d0 = w[0] - ub[0], d1 = w[1] - ub[1], d2 = w[2] - ub[2], d3 = w[3] - ub[3];
+    const double a = d3 * d0 - 0.5 * (d1 * d1 + d2 * d2);
+    const double b = ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0;
+    // h > 0 for every t > 0 when it starts increasing and curves up
+    if (a >= 0.0 && b >= 0.0) continue;
+    const double disc = b * b - 4.0 * a * c;
+    if (disc < 0.0) continue;
+    const double q = -0.5 * (b + copysign(sqrt(disc), b));
+    const double r1 = a != 0.0 ? q / a : 1e300, r2 = q != 0.0 ? c / q : 1e300;
+    const double p1 = r1 > 0.0 ? r1 : 1e300, p2 = r2 > 0.0 ? r2 : 1e300;
+    const double t = p1 < p2 ? p1 : p2;
+    tstar = t < tstar ? t : tstar;
   }
 }
 
@@ -155,8 +201,8 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
     const double p_lo = (g - 1.0) * (ub[3] - lam * dev[3] - 0.5 * m_hi * m_hi / rho_lo);
     if (p_lo >= eps_p) return;
   }
-  double rmin, pmin;
-  probe_minima<K, P>(u, ub, 1.0, true, g, rmin, pmin);
+  double rmin, pmin, tstar;
+  probe_scan<K, P>(u, ub, eps_p, g, rmin, pmin, tstar);
   if (!(rmin < eps_r) && !(pmin < eps_p)) return;
 
   double theta = 1.0;
@@ -165,15 +211,23 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
     theta = (ub[0] - eps_r) / (gap > 0.0 ? gap : 1.0);
     theta = theta < 0.0 ? 0.0 : (theta > 1.0 ? 1.0 : theta);
   }
-  double r_unused, p_hi;
-  probe_minima<K, P>(u, ub, theta, false, g, r_unused, p_hi);
-  if (!(p_hi >= eps_p)) {
+  // The reference bisects on min_x p(ubar + t (u(x) - ubar)) >= eps_p over
+  // [0, theta] (12 steps, src/spatial/limiter.py:151-178).  p is concave along
+  // the segment, so that test is exactly "t <= t*" for one t* per element, and
+  // t* is the smallest positive root over the probe points of the quadratic
+  // rho(t) (p(t) - eps_p).  The probe scan above found t*; the bisection is then
+  // replayed on the scalar t* with the reference's own midpoints.  A decision
+  // within 1e-7 theta of t* -- where the root's rounding could disagree with
+  // the reference's pointwise arithmetic -- is taken with that arithmetic.
+  auto admissible = [&](double t) -> bool {
+    if (fabs(t - tstar) > 1e-7 * theta) return t < tstar;
+    return pmin_at<K, P>(u, ub, t, g) >= eps_p;
+  };
+  if (!admissible(theta)) {
     double lo = 0.0, hi = theta;
     for (int it = 0; it < ph.lim_steps; ++it) {
       const double mid = 0.5 * (lo + hi);
-      double pm;
-      probe_minima<K, P>(u, ub, mid, false, g, r_unused, pm);
-      if (pm >= eps_p)
+      if (admissible(mid))
         lo = mid;
       else
         hi = mid;
@@ -210,7 +264,10 @@ struct Launch {
   static constexpr int NT = (NP * 4 * 8 * 128 <= 40 * 1024) ? 128 : 64;
 };
 
-template <int K, int P, bool AFF>
+// LIM = false compiles the residual / rate variant, without the stage update
+// and the limiter (a smaller kernel: fewer registers, no instruction-cache
+// pressure from code it never runs); LIM = true handles stages and the limiter.
+template <int K, int P, bool AFF, bool LIM>
 __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, const nzb_physics ph, const Work w) {
   using S = Shape<K, P>;
   constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
@@ -225,13 +282,13 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
   double nrm = 0.0;
   int scaled = 0, repaired = 0;
 
-  if (active && w.op == OP_LIMIT) {
+  if (LIM && active && w.op == OP_LIMIT) {
     double u[NP][4];
 #pragma unroll
     for (int i = 0; i < NP; ++i)
 #pragma unroll
       for (int s = 0; s < 4; ++s) u[i][s] = w.V[(s * NP + i) * E + e];
-    if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
+    if (LIM && ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
 #pragma unroll
     for (int i = 0; i < NP; ++i)
 #pragma unroll
@@ -269,45 +326,60 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
       const double len = __ldg(m.edge_geo + 4 * (int64_t)k + 3);
       double ue[NE][4], un[NE][4];
       int node[NE];
-#pragma unroll
-      for (int j = 0; j < NE; ++j) {
-        node[j] = edge_node(K, P, f, j);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) ue[j][s] = __ldg(w.V + (s * NP + node[j]) * E + e);
-      }
-      if (nb >= 0) {
-        // the neighbour's edge coefficients in the edge's (owner's) orientation
+      if (AFF) {
 #pragma unroll
         for (int j = 0; j < NE; ++j) {
-          const int n = edge_node(K, P, nf, side ? j : NE - 1 - j);
+          node[j] = edge_node(K, P, f, j);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) un[j][s] = __ldg(w.V + (s * NP + n) * E + nb);
+          for (int s = 0; s < 4; ++s) ue[j][s] = __ldg(w.V + (s * NP + node[j]) * E + e);
+        }
+        if (nb >= 0) {
+          // the neighbour's edge coefficients in the edge's (owner's) orientation
+#pragma unroll
+          for (int j = 0; j < NE; ++j) {
+            const int n = edge_node(K, P, nf, side ? j : NE - 1 - j);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) un[j][s] = __ldg(w.V + (s * NP + n) * E + nb);
+          }
         }
       }
       const double coef = (side ? -1.0 : 1.0) * fs;
       double smax = 0.0;
 #pragma unroll 1
       for (int q = 0; q < NQF; ++q) {
-        // side 1 walks the edge backwards: l_j(1 - sigma_q) = l_{p-j}(sigma_q)
-        double cj[NE], lj[NE];
+        double tc[4] = {0.0, 0.0, 0.0, 0.0}, tn[4] = {0.0, 0.0, 0.0, 0.0};
+        double cj[NE];
+        // general geometry: the reference's full face basis phi_face[side, f]
+        const int own = S::O_PF + ((side * NF + f) * NP) * NQF + q;
+        if (AFF) {
+          // side 1 walks the edge backwards: l_j(1 - sigma_q) = l_{p-j}(sigma_q)
 #pragma unroll
-        for (int j = 0; j < NE; ++j) {
-          lj[j] = c_tab[S::O_E1D + j * NQF + q];
-          const double r = c_tab[S::O_E1D + (NE - 1 - j) * NQF + q];
-          cj[j] = side ? r : lj[j];
+          for (int j = 0; j < NE; ++j) {
+            const double l = c_tab[S::O_E1D + j * NQF + q];
+            const double r = c_tab[S::O_E1D + (NE - 1 - j) * NQF + q];
+            cj[j] = side ? r : l;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+              tc[s] = fma(cj[j], ue[j][s], tc[s]);
+              if (nb >= 0) tn[s] = fma(l, un[j][s], tn[s]);
+            }
+          }
+        } else {
+          const int oth = S::O_PF + (((1 - side) * NF + nf) * NP) * NQF + q;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double b = c_tab[own + i * NQF];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) tc[s] = fma(b, __ldg(w.V + (s * NP + i) * E + e), tc[s]);
+            if (nb >= 0) {
+              const double bn = c_tab[oth + i * NQF];
+#pragma unroll
+              for (int s = 0; s < 4; ++s) tn[s] = fma(bn, __ldg(w.V + (s * NP + i) * E + nb), tn[s]);
+            }
+          }
         }
-        double tc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < NE; ++j)
-#pragma unroll
-          for (int s = 0; s < 4; ++s) tc[s] = fma(cj[j], ue[j][s], tc[s]);
         double F[4], sp;
         if (nb >= 0) {
-          double tn[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-          for (int j = 0; j < NE; ++j)
-#pragma unroll
-            for (int s = 0; s < 4; ++s) tn[s] = fma(lj[j], un[j][s], tn[s]);
           double L[4], R[4];
 #pragma unroll
           for (int s = 0; s < 4; ++s) {
@@ -323,13 +395,25 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
         double fwc[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) fwc[s] = (F[s] * scale) * coef;
+        if (AFF) {
 #pragma unroll
-        for (int j = 0; j < NE; ++j)
+          for (int j = 0; j < NE; ++j)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            double& a = facc[(node[j] * 4 + s) * BT + t];
-            a = fma(cj[j], fwc[s], a);
+            for (int s = 0; s < 4; ++s) {
+              double& a = facc[(node[j] * 4 + s) * BT + t];
+              a = fma(cj[j], fwc[s], a);
+            }
+        } else {
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double b = c_tab[own + i * NQF];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+              double& a = facc[(i * 4 + s) * BT + t];
+              a = fma(b, fwc[s], a);
+            }
           }
+        }
       }
       wave += smax * len;
     }
@@ -356,7 +440,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
 #pragma unroll
           for (int s = 0; s < 4; ++s) uq[s] = fma(phi, u[i][s], uq[s]);
         }
-        const Prim pr = primitives(uq, g);
+        const Prim pr = primitives_fast(uq, g);
         const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
         const double G[4] = {pr.rho * pr.vy, pr.rho * pr.vx * pr.vy, pr.rho * pr.vy * pr.vy + pr.p, pr.rho * pr.vy * pr.H};
         if (AFF) {
@@ -392,7 +476,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
         for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = acc[i][s];
     } else {
       double dt = 0.0;
-      if (w.op == OP_STAGE) {
+      if (LIM && w.op == OP_STAGE) {
         if (w.stage == 1) {
           const double d = wave < FLOOR ? FLOOR : wave;
           dt = w.dt_factor * 2.0 * __ldg(m.area + e) / d;
@@ -401,12 +485,13 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
           dt = w.dt[e];
         }
       }
-      // rate = -M^-1 R, consumed row by row; the stage update overwrites u
+      // rate = -M^-1 R, one component at a time so its accumulators retire as
+      // the new state is formed
       double u[NP][4];
 #pragma unroll
-      for (int i = 0; i < NP; ++i) {
+      for (int s = 0; s < 4; ++s) {
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
+        for (int i = 0; i < NP; ++i) {
           double r = 0.0;
           if (AFF) {
 #pragma unroll
@@ -416,7 +501,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
             for (int j = 0; j < NP; ++j) r = fma(__ldg(m.minv + (i * NP + j) * E + e), acc[j][s], r);
             r = -r;
           }
-          if (w.op == OP_RATE) {
+          if (!LIM || w.op == OP_RATE) {
             w.out[(s * NP + i) * E + e] = r;
           } else {
             const double v = __ldg(w.V + (s * NP + i) * E + e);
@@ -431,7 +516,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
           }
         }
       }
-      if (w.op == OP_STAGE) {
+      if (LIM && w.op == OP_STAGE) {
         if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
 #pragma unroll
         for (int i = 0; i < NP; ++i)
@@ -442,8 +527,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
     }
   }
   // block-level reductions (every thread of the block reaches these)
-  if (w.op == OP_STAGE && w.norm_partial && w.stage == 1) block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
-  if ((w.op == OP_STAGE || w.op == OP_LIMIT) && w.counters) {
+  if (LIM && w.op == OP_STAGE && w.norm_partial && w.stage == 1) block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
+  if (LIM && (w.op == OP_STAGE || w.op == OP_LIMIT) && w.counters) {
     const int ns = __syncthreads_count(scaled);
     const int nr = __syncthreads_count(repaired);
     if (t == 0) {

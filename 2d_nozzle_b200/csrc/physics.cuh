@@ -36,6 +36,20 @@ __device__ __forceinline__ Prim primitives(const double* U, double g) {
   return s;
 }
 
+// The same primitives with one division: vx = U1 (1/rho) differs from U1 / rho
+// in the last bit at most.  Used for the volume-point fluxes, which feed only
+// the weak-form projection, never a branch.
+__device__ __forceinline__ Prim primitives_fast(const double* U, double g) {
+  Prim s;
+  s.rho = floor_at(U[0], FLOOR);
+  const double inv = 1.0 / s.rho;
+  s.vx = U[1] * inv;
+  s.vy = U[2] * inv;
+  s.p = floor_at((g - 1.0) * (U[3] - 0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy)), FLOOR);
+  s.H = (U[3] + s.p) * inv;
+  return s;
+}
+
 __device__ __forceinline__ void normal_flux(const Prim& s, double nx, double ny, double* F) {
   const double vn = s.vx * nx + s.vy * ny;
   F[0] = s.rho * vn;

@@ -44,7 +44,9 @@ def element_tables(ref) -> np.ndarray:
     e1d = np.asarray(ref.phi_face)[0, f0][nodes, :]
     wf = np.asarray(ref.w_face)
     mw = (phi @ w) / w.sum()
-    return np.ascontiguousarray(np.concatenate([phi.ravel(), wxi.ravel(), weta.ravel(), minv.ravel(), e1d.ravel(), wf, mw]))
+    pf = np.asarray(ref.phi_face)  # (2, NF, NP, NQF)
+    return np.ascontiguousarray(np.concatenate([phi.ravel(), wxi.ravel(), weta.ravel(), minv.ravel(), e1d.ravel(), wf, mw,
+                                                pf.ravel()]))
 
 
 def lebesgue_constant(ref) -> float:

@@ -1,0 +1,78 @@
+"""The C ABI library loads and exports every function include/*.h declares (no device calls)."""
+
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import re
+import types
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, pkg
+
+
+def declared_functions() -> set[str]:
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\b(nzb_\w+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    path = pkg("build").build()
+    return ctypes.CDLL(path)
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_the_header():
+    bound = {n for n, _, _ in pkg("capi").SIGNATURES}
+    assert declared_functions() <= bound
+
+
+def test_table_sizes_agree_with_the_packer():
+    capi, layout, re_ = pkg("capi"), pkg("layout"), pkg("refelem")
+    lib = capi.load()
+    for kind, k in (("tri", 0), ("quad", 1)):
+        for p in range(4):
+            tab = layout.element_tables(re_.ref_tables(kind, p))
+            assert lib.nzb_table_size(k, p) == tab.size
+    assert lib.nzb_table_size(0, 4) == -1
+    assert lib.nzb_version() == 1
+
+
+def test_struct_layouts_match_the_header():
+    capi = pkg("capi")
+    # 4 x int32 + 2 x int64 + 10 pointers
+    assert ctypes.sizeof(capi.Mesh) == 16 + 16 + 10 * 8
+    assert ctypes.sizeof(capi.Physics) == 3 * 8 + 8 + 9 * 8 + 4 * 8 + 8 + 4 * 8
+    assert ctypes.sizeof(capi.StageArgs) == 7 * 8 + 3 * 8 + 8
+
+
+def test_lebesgue_constant_bounds_probe_values():
+    layout, re_ = pkg("layout"), pkg("refelem")
+    for kind, p, expect in (("tri", 3, 2.031), ("quad", 3, 2.133), ("tri", 1, 1.0)):
+        assert abs(layout.lebesgue_constant(re_.ref_tables(kind, p)) - expect) < 1e-3
+
+
+def test_physics_struct_constants():
+    layout, cfg, re_ = pkg("layout"), pkg("config"), pkg("refelem")
+    flow = cfg.FlowConditions(flux="hllc", backflow=True)
+    ph = layout.physics_struct(flow, cfg.SolverOptions(), re_.ref_tables("tri", 1))
+    assert ph.flux == 1 and ph.limiter == 1
+    assert ph.in_rho_t == pytest.approx(2.5) and ph.bf_rho_t == pytest.approx(2.5)
+    assert ph.p_back == pytest.approx(0.15)
+    assert list(ph.norm_w) == pytest.approx([1.0, 1 / 0.7483314773547883, 1 / 0.7483314773547883, 1 / 0.56])
+    with pytest.raises(NotImplementedError):
+        layout.physics_struct(types.SimpleNamespace(flux="slau2"), cfg.SolverOptions(), None)

@@ -1,0 +1,125 @@
+"""CUDA path vs the reference's fixtures and the CPU oracle (through the C ABI).
+
+Tolerances are the reference tests' normwise metric max|a-b|/max|b|:
+1e-12 for residuals, rates and states (the reference pins numba vs numpy at
+1e-10 with fastmath); limited-element sets must be identical.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import TINY, golden, pkg, rel, tiny_ops
+from oracle import dg_oracle as orc
+
+pytestmark = pytest.mark.gpu
+FLUXES = ("roe", "hllc", "ausmup")
+TOL = 1e-12
+
+
+def backend(ops, flow=None, opts=None, **kw):
+    cfg = pkg("config")
+    return pkg("backend").B200Backend(ops, flow or cfg.FlowConditions(), opts or cfg.SolverOptions(), **kw)
+
+
+def geometries(kind):
+    return (False, True) if kind == "tri" else (True,)
+
+
+@pytest.mark.parametrize("kind,p", TINY)
+@pytest.mark.parametrize("flux", FLUXES)
+def test_residual_rate_wave(cuda, kind, p, flux):
+    ops, g = tiny_ops(kind, p)
+    flow = pkg("config").FlowConditions(flux=flux)
+    for general in geometries(kind):
+        bk = backend(ops, flow, force_general=general)
+        R, wave = bk.residual(g["U"])
+        F, wave2 = bk.rate(g["U"])
+        assert rel(R, g[f"R_{flux}"]) < TOL
+        assert rel(wave, g[f"wave_{flux}"]) < TOL and rel(wave2, g[f"wave_{flux}"]) < TOL
+        assert rel(F, g[f"rate_{flux}"]) < TOL
+        assert rel(F, orc.rate(g["U"], ops, flow)[0]) < TOL
+
+
+@pytest.mark.parametrize("kind,p", TINY)
+def test_backflow_and_inverse_mass(cuda, kind, p):
+    ops, g = tiny_ops(kind, p)
+    bk = backend(ops, pkg("config").FlowConditions(backflow=True))
+    R, _ = bk.residual(g["U"])
+    assert rel(R, g["R_roe_backflow"]) < TOL
+    assert rel(bk.inverse_mass(R), orc.inverse_mass(R, ops)) < TOL
+
+
+@pytest.mark.parametrize("kind,p", TINY)
+def test_limiter_values_and_sets(cuda, kind, p):
+    ops, g = tiny_ops(kind, p)
+    bk = backend(ops)
+    out, flags = bk.limit_flags(g["U_bad"])
+    ref, bad, rep = orc.positivity(g["U_bad"], ops, bk.flow)
+    assert rel(out, g["limited_bad"]) < TOL
+    assert np.array_equal(flags & 1 > 0, bad)
+    assert np.array_equal(flags & 2 > 0, rep)
+
+
+@pytest.mark.parametrize("kind,p", TINY)
+@pytest.mark.parametrize("scheme", ["euler", "ssprk3"])
+def test_three_steps(cuda, kind, p, scheme):
+    ops, g = tiny_ops(kind, p)
+    bk = backend(ops, opts=pkg("config").SolverOptions(scheme=scheme))
+    V, res = bk.run(g["U"].copy(), 3, scheme)
+    assert rel(V, g[f"run3_{scheme}"]) < TOL
+    assert abs(res - g[f"run3_{scheme}_res"]) <= 1e-12 * abs(g[f"run3_{scheme}_res"])
+
+
+def test_chunked_runs_agree_and_do_not_alias(cuda):
+    ops, g = tiny_ops("tri", 1)
+    bk = backend(ops)
+    once, _ = bk.run(g["U"].copy(), 6, "ssprk3")
+    half, _ = bk.run(g["U"].copy(), 3, "ssprk3")
+    twice, _ = bk.run(half, 3, "ssprk3")
+    assert np.array_equal(once, twice)
+    kept = once.copy()
+    bk.run(g["U"].copy(), 4, "ssprk3")
+    assert np.array_equal(once, kept)
+
+
+@pytest.mark.parametrize("flux", FLUXES)
+def test_microbench_distribution(cuda, flux):
+    """Config-2 states (lognormal density and pressure, Mach 0.2-3) on 400 cubic triangles."""
+    g = golden("rect_tri_p3.npz")
+    topo, _, _ = pkg("mesh").channel_topology("tri", nx=20, nr=10)
+    ops = pkg("operators").build_operators(topo, g["node_coords"], 3)
+    cfg = pkg("config")
+    bk = backend(ops, cfg.FlowConditions(flux=flux), cfg.SolverOptions(cfl=0.5))
+    R, wave = bk.residual(g["U"])
+    assert rel(R, g[f"R_{flux}"]) < TOL and rel(wave, g[f"wave_{flux}"]) < TOL
+    V, res, flags = bk.step_record(g["U"].copy())
+    assert rel(V, g[f"step_{flux}"]) < TOL
+    assert abs(res - g[f"step_{flux}_res"]) <= 1e-12 * g[f"step_{flux}_res"]
+    assert np.array_equal(flags & 1 > 0, g[f"step_{flux}_limited"])
+    run, res2 = bk.run(g["U"].copy(), 1, "ssprk3")
+    assert np.array_equal(run, V) and res2 == res
+
+
+def test_shocked_quads_fixed_steps(cuda):
+    """Config 3 (conical AR 3, cubic quads, refine 3, HLLC, pb 0.6): five steps, stage by stage."""
+    g = golden("config3.npz")
+    topo, _, _ = pkg("mesh").channel_topology("quad", refine=3)
+    ops = pkg("operators").build_operators(topo, g["node_coords"], 3)
+    cfg = pkg("config")
+    bk = backend(ops, cfg.FlowConditions(flux="hllc", back_pressure_ratio=0.6, allow_shock_in_nozzle=True))
+    U, ress, masks = g["U0"].copy(), [], []
+    for _ in range(int(g["n_steps"])):
+        U, res, flags = bk.step_record(U)
+        ress.append(res)
+        masks.extend(list(flags & 1 > 0))
+    assert rel(U, g["U_final"]) < TOL
+    assert np.abs(np.array(ress) - g["res"]).max() <= 1e-12 * np.abs(g["res"]).max()
+    assert np.array_equal(np.stack(masks), g["limited"])
+
+
+def test_norm_matches_the_oracle(cuda):
+    ops, g = tiny_ops("tri", 3)
+    bk = backend(ops)
+    assert abs(bk.norm(g["U"]) - orc.norm(g["U"], bk.flow)) <= 1e-14 * orc.norm(g["U"], bk.flow)
