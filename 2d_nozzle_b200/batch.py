@@ -1,0 +1,217 @@
+"""Batched steady solves: many independent design points marched together.
+
+A sweep's points have uneven meshes (element kind, order and refinement vary),
+so the instances are grouped into buckets of one (kind, order); each bucket's
+elements are concatenated, with connectivity offset, into one device mesh, and
+each SSP-RK3 stage is one kernel launch per bucket over every instance in it.
+An ``elem_inst`` array maps elements to instances, which carry their own back
+pressure, tolerance and march state.  After every chunk (one step first, then
+``check_interval`` steps, as the reference's march does) a device kernel
+evaluates each running instance's residual and applies the reference's
+convergence, non-finite, divergence, stall and iteration-cap tests
+(src/timestepping/march.py:125-230); retired instances are no longer advanced,
+so every instance ends on exactly the iteration the one-at-a-time march would.
+Each chunk is one CUDA graph; the host reads one integer (the number of
+instances still running) per chunk.
+
+This replaces the reference's serial, warm-started ``sweep`` loop
+(src/sweep.py:300-446) for the solve itself; refusal of shocked operating
+points happens on the host before batching, as there.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+from .config import FLUX_IDS, SCHEMES, recommended_scheme, residual_scale, step_coefficient
+from .layout import DeviceMesh, concat_arrays, host_arrays, physics_struct
+
+STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "diverged", 4: "stalled", 5: "max_iterations"}
+
+
+@dataclass
+class Instance:
+    ops: object
+    flow: object
+    opts: object
+    U0: np.ndarray
+    length: float = 1.0
+
+
+@dataclass
+class InstanceResult:
+    status: str
+    converged: bool
+    iterations: int
+    residual: float
+    residual_initial: float
+    U: np.ndarray | None
+
+
+class BatchSolver:
+    def __init__(self, instances: list[Instance], device=None):
+        import torch
+
+        if not instances:
+            raise ValueError("empty batch")
+        self.torch = torch
+        self.lib = capi.load()
+        self.instances = instances
+        opts0 = instances[0].opts
+        for inst in instances:
+            o = inst.opts
+            if (o.cfl, o.limiter, o.check_interval, o.max_iterations, o.stall_window, o.stall_ratio,
+                    o.divergence_factor, o.scheme, getattr(o, "positivity_cfl", 0.0)) != (
+                    opts0.cfl, opts0.limiter, opts0.check_interval, opts0.max_iterations, opts0.stall_window,
+                    opts0.stall_ratio, opts0.divergence_factor, opts0.scheme, getattr(opts0, "positivity_cfl", 0.0)):
+                raise ValueError("every instance of a batch must share the march options")
+            if inst.flow.flux not in FLUX_IDS:
+                raise NotImplementedError(f"flux {inst.flow.flux!r}")
+        self.opts = opts0
+        dev = torch.device(device if device is not None else "cuda")
+        self.device = dev
+        n = len(instances)
+
+        # buckets of one (kind, order)
+        keys = [(inst.ops.ref.kind, inst.ops.ref.order) for inst in instances]
+        self.bucket_keys = sorted(set(keys), key=lambda k: (k[0], k[1]))
+        self.members = [[i for i in range(n) if keys[i] == k] for k in self.bucket_keys]
+        begin = np.zeros(n, np.int64)
+        end = np.zeros(n, np.int64)
+        local = np.zeros(n, np.int64)
+        count = np.zeros(n)
+        tol = np.zeros(n)
+        p_back = np.zeros(n)
+        self.meshes, self.buffers, self.phys, self.offsets, self.factors = [], [], [], [], []
+        self._keep = []
+        g_off = 0
+        for key, mem in zip(self.bucket_keys, self.members):
+            parts = [host_arrays(instances[i].ops) for i in mem]
+            arrays = concat_arrays(parts)
+            ref = instances[mem[0]].ops.ref
+            dm = DeviceMesh(device=dev, arrays=arrays, ref=ref)
+            flow0 = instances[mem[0]].flow
+            for i in mem:
+                f = instances[i].flow
+                if (f.gamma, f.flux, f.entropy_fix, f.hllc_low_mach, f.backflow, f.total_pressure,
+                        f.total_temperature, f.Rgas, f.inflow_angle) != (flow0.gamma, flow0.flux, flow0.entropy_fix,
+                                                                          flow0.hllc_low_mach, flow0.backflow,
+                                                                          flow0.total_pressure, flow0.total_temperature,
+                                                                          flow0.Rgas, flow0.inflow_angle):
+                    raise ValueError("instances of a bucket may differ only in back pressure")
+            ph = physics_struct(flow0, opts0, ref)
+            elem_inst = np.empty(arrays["n_elem"], np.int32)
+            l_off = 0
+            for i, part in zip(mem, parts):
+                E_i = part["n_elem"]
+                elem_inst[l_off:l_off + E_i] = i
+                begin[i], end[i], local[i] = g_off + l_off, g_off + l_off + E_i, l_off
+                count[i] = 4.0 * E_i * ref.n_basis
+                f = instances[i].flow
+                tol[i] = opts0.tolerance * residual_scale(f, instances[i].length)
+                p_back[i] = f.back_pressure
+                l_off += E_i
+            self._keep.append(torch.as_tensor(elem_inst, device=dev))
+            dm.elem_inst_t = self._keep[-1]
+            S = [dm.state() for _ in range(3)]
+            dt = torch.zeros(dm.E, dtype=torch.float64, device=dev)
+            U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])
+            dm.pack(U0, S[0])
+            bf = capi.Buffers()
+            bf.S0, bf.S1, bf.S2 = (x.data_ptr() for x in S)
+            bf.dt = dt.data_ptr()
+            self._keep += S + [dt]
+            scheme = opts0.scheme or recommended_scheme(ref.order)
+            if scheme not in SCHEMES:
+                raise ValueError(f"unknown scheme {scheme!r}")
+            pc = getattr(opts0, "positivity_cfl", 0.0)
+            pscale = float(pc) if (pc > 0.0 and opts0.limiter != "none" and ref.order > 0) else 1.0
+            if (scheme == "ssprk3") != (ref.order > 0):
+                raise NotImplementedError("batches march SSP-RK3 above p = 0 and forward Euler at p = 0")
+            self.meshes.append(dm)
+            self.buffers.append((bf, S))
+            self.phys.append(ph)
+            self.offsets.append(g_off)
+            self.factors.append(pscale * step_coefficient(ref.order, opts0.cfl, scheme))
+            g_off += dm.E
+        self.n_elem = g_off
+        self.begin, self.end, self.local = begin, end, local
+
+        T = lambda a, dt: torch.as_tensor(a, dtype=dt, device=dev)  # noqa: E731
+        W = opts0.stall_window
+        self.t = {
+            "begin": T(begin, torch.int64), "end": T(end, torch.int64), "count": T(count, torch.float64),
+            "tol": T(tol, torch.float64), "p_back": T(p_back, torch.float64),
+            "elem_norm": torch.zeros(g_off, dtype=torch.float64, device=dev),
+            "status": torch.zeros(n, dtype=torch.int32, device=dev), "iterations": torch.zeros(n, dtype=torch.int32, device=dev),
+            "res0": torch.zeros(n, dtype=torch.float64, device=dev), "res": torch.zeros(n, dtype=torch.float64, device=dev),
+            "window": torch.zeros(n * W, dtype=torch.float64, device=dev),
+            "window_count": torch.zeros(n, dtype=torch.int32, device=dev),
+            "n_running": torch.zeros(1, dtype=torch.int32, device=dev),
+        }
+        for dm in self.meshes:
+            dm.set_batch(dm.elem_inst_t, self.t["status"], self.t["p_back"])
+        bm = capi.BatchMarch()
+        bm.n_inst = n
+        for f, k in (("inst_begin", "begin"), ("inst_end", "end"), ("inst_count", "count"), ("inst_tol", "tol"),
+                     ("elem_norm", "elem_norm"), ("status", "status"), ("iterations", "iterations"), ("res0", "res0"),
+                     ("res", "res"), ("window", "window"), ("window_count", "window_count"), ("n_running", "n_running")):
+            setattr(bm, f, self.t[k].data_ptr())
+        bm.divergence_factor = float(opts0.divergence_factor)
+        bm.stall_ratio = float(opts0.stall_ratio)
+        bm.stall_window = int(W)
+        bm.max_iterations = int(opts0.max_iterations)
+        self.bm = bm
+        nb = len(self.meshes)
+        meshes = (capi.Mesh * nb)(*[dm.c for dm in self.meshes])
+        physs = (capi.Physics * nb)(*self.phys)
+        bufs = (capi.Buffers * nb)(*[b for b, _ in self.buffers])
+        offs = np.asarray(self.offsets, np.int64)
+        facs = np.asarray(self.factors, float)
+        h = capi.P()
+        capi.check(self.lib.nzb_batch_create(nb, meshes, physs, bufs, offs.ctypes.data, facs.ctypes.data, C.byref(bm),
+                                             C.byref(h)), "nzb_batch_create")
+        self.handle = h.value
+        self.done = 0
+        self.chunks = 0
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.lib.nzb_batch_destroy(self.handle)
+
+    @property
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.device).cuda_stream
+
+    def step_chunk(self, n: int, first: bool) -> int:
+        capi.check(self.lib.nzb_batch_run(self.handle, int(n), 1 if first else 0, self._stream), "nzb_batch_run")
+        self.done += n
+        self.chunks += 1
+        return int(self.t["n_running"].item())
+
+    def run(self) -> int:
+        """March every instance to retirement; returns the number of chunks."""
+        o = self.opts
+        running = self.step_chunk(1, True)
+        chunk = min(max(1, o.check_interval), o.max_iterations)
+        while running and self.done < o.max_iterations:
+            running = self.step_chunk(min(chunk, o.max_iterations - self.done), False)
+        return self.chunks
+
+    def results(self, with_state: bool = True) -> list[InstanceResult]:
+        st = self.t["status"].cpu().numpy()
+        its = self.t["iterations"].cpu().numpy()
+        res = self.t["res"].cpu().numpy()
+        res0 = self.t["res0"].cpu().numpy()
+        states = {}
+        if with_state:
+            for dm, (bf, S), mem in zip(self.meshes, self.buffers, self.members):
+                full = dm.unpack(S[0]).cpu().numpy()
+                for i in mem:
+                    states[i] = full[self.local[i]:self.local[i] + self.instances[i].ops.n_elem]
+        return [InstanceResult(STATUS[int(st[i])], int(st[i]) == 1, int(its[i]), float(res[i]), float(res0[i]),
+                               states.get(i)) for i in range(len(self.instances))]

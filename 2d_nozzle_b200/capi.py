@@ -27,15 +27,15 @@ class Mesh(C.Structure):
         ("n_elem", I64),
         ("n_edge", I64),
         ("geo", P),
-        ("gx", P),
-        ("gy", P),
         ("minv", P),
-        ("mean_w", P),
         ("area", P),
         ("face_nbr", P),
         ("face_code", P),
         ("face_edge", P),
         ("edge_geo", P),
+        ("elem_inst", P),
+        ("inst_status", P),
+        ("inst_p_back", P),
     ]
 
 
@@ -72,6 +72,7 @@ class StageArgs(C.Structure):
         ("out", P),
         ("dt", P),
         ("norm_partial", P),
+        ("elem_norm", P),
         ("counters", P),
         ("flags", P),
         ("dt_factor", C.c_double),
@@ -94,6 +95,28 @@ class Buffers(C.Structure):
     ]
 
 
+class BatchMarch(C.Structure):
+    _fields_ = [
+        ("n_inst", I64),
+        ("inst_begin", P),
+        ("inst_end", P),
+        ("inst_count", P),
+        ("inst_tol", P),
+        ("elem_norm", P),
+        ("status", P),
+        ("iterations", P),
+        ("res0", P),
+        ("res", P),
+        ("window", P),
+        ("window_count", P),
+        ("n_running", P),
+        ("divergence_factor", C.c_double),
+        ("stall_ratio", C.c_double),
+        ("stall_window", I32),
+        ("max_iterations", I32),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol
 SIGNATURES = [
     ("nzb_version", C.c_int, []),
@@ -113,6 +136,10 @@ SIGNATURES = [
     ("nzb_solver_create", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(Buffers), C.c_int, C.c_double, C.POINTER(P)]),
     ("nzb_solver_run", C.c_int, [P, C.c_int, P]),
     ("nzb_solver_destroy", C.c_int, [P]),
+    ("nzb_batch_create", C.c_int, [C.c_int, C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(Buffers), P, P,
+                                   C.POINTER(BatchMarch), C.POINTER(P)]),
+    ("nzb_batch_run", C.c_int, [P, C.c_int, C.c_int, P]),
+    ("nzb_batch_destroy", C.c_int, [P]),
 ]
 
 _lib = None

@@ -12,6 +12,7 @@
 #include <set>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "element.cuh"
 #include "nozzle_b200.h"
@@ -50,8 +51,8 @@ static int check_mesh(const nzb_mesh* m) {
   if (m->n_elem <= 0) return fail("mesh has no elements");
   if (!m->area || !m->face_nbr || !m->face_code || !m->face_edge || !m->edge_geo)
     return fail("mesh arrays area/face_nbr/face_code/face_edge/edge_geo are required");
-  if (m->affine ? !m->geo : (!m->gx || !m->gy || !m->minv || !m->mean_w))
-    return fail(m->affine ? "affine mesh needs geo" : "general mesh needs gx, gy, minv, mean_w");
+  if (!m->geo || (!m->affine && !m->minv))
+    return fail(m->affine ? "affine mesh needs geo" : "general mesh needs geo (vertices) and minv");
   if (!tables_ready(m->kind, m->order)) return fail("reference tables not uploaded for this kind/order on this device");
   return 0;
 }
@@ -274,6 +275,163 @@ static int graph_for(Solver& s, int n, cudaGraphExec_t* out) {
   return 0;
 }
 
+// ---- batched march ----------------------------------------------------------------
+// Copy S1 -> S0 for the elements of running instances (forward Euler in a batch).
+__global__ void k_masked_copy(const double* __restrict__ src, double* __restrict__ dst, int64_t E, int np,
+                              const int32_t* __restrict__ elem_inst, const int32_t* __restrict__ status) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * np * 4) return;
+  const int64_t e = t % E;
+  if (elem_inst && status[elem_inst[e]] != 0) return;
+  dst[t] = src[t];
+}
+
+// One block per instance: the weighted RMS of its last stage-1 rate, summed in a
+// fixed order, then the reference march's tests (src/timestepping/march.py:
+// 157-220) on that residual.
+__global__ void __launch_bounds__(256) k_batch_check(nzb_batch_march bm, int n_steps, int first) {
+  const int64_t inst = blockIdx.x;
+  if (inst >= bm.n_inst || bm.status[inst] != 0) return;
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int64_t e = bm.inst_begin[inst] + threadIdx.x; e < bm.inst_end[inst]; e += 256) acc += bm.elem_norm[e];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double res = sqrt(red[0] / bm.inst_count[inst]);
+  const int done = bm.iterations[inst] + n_steps;
+  bm.iterations[inst] = done;
+  bm.res[inst] = res;
+  int st = 0;
+  if (first) {
+    bm.res0[inst] = res;
+    if (!isfinite(res))
+      st = 2;
+    else if (res <= bm.inst_tol[inst])
+      st = 1;
+  } else if (!isfinite(res)) {
+    st = 2;
+  } else if (res <= bm.inst_tol[inst]) {
+    st = 1;
+  } else if (res > bm.divergence_factor * bm.res0[inst]) {
+    st = 3;
+  } else {
+    const int W = bm.stall_window;
+    const int c = bm.window_count[inst];
+    bm.window[inst * W + (c % W)] = res;
+    bm.window_count[inst] = c + 1;
+    if (c + 1 >= W) {
+      double best = 1e300, worst = -1e300;
+      for (int k = 0; k < W; ++k) {
+        const double v = bm.window[inst * W + k];
+        best = v < best ? v : best;
+        worst = v > worst ? v : worst;
+      }
+      if (worst > 0.0 && best / worst > bm.stall_ratio) st = 4;
+    }
+  }
+  if (st == 0 && done >= bm.max_iterations) st = 5;
+  bm.status[inst] = st;
+  if (st == 0) atomicAdd(bm.n_running, 1);
+}
+
+struct Batch {
+  std::vector<nzb_mesh> mesh;
+  std::vector<nzb_physics> phys;
+  std::vector<nzb_buffers> buf;
+  std::vector<int64_t> offset;
+  std::vector<double> factor;
+  nzb_batch_march bm;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // buckets march concurrently: one capture stream and join event per bucket
+  std::vector<cudaStream_t> bstream;
+  std::vector<cudaEvent_t> bdone;
+  cudaEvent_t fork = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;  // key: 2 * n + first
+};
+
+static int enqueue_bucket_step(const Batch& B, size_t b, cudaStream_t st) {
+  {
+    const nzb_mesh& m = B.mesh[b];
+    const nzb_buffers& bf = B.buf[b];
+    const bool ssp = m.order > 0;
+    Work w{};
+    w.op = OP_STAGE;
+    w.dt = bf.dt;
+    w.dt_factor = B.factor[b];
+    w.V = bf.S0;
+    w.out = ssp ? bf.S2 : bf.S1;
+    w.elem_norm = B.bm.elem_norm + B.offset[b];
+    w.stage = 1;
+    w.a = 0.0;
+    w.b = 1.0;
+    if (dispatch(m, B.phys[b], w, st)) return -1;
+    if (!ssp) {
+      const int np = n_basis(m.kind, m.order);
+      const int64_t n = m.n_elem * np * 4;
+      k_masked_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(bf.S1, bf.S0, m.n_elem, np, m.elem_inst, m.inst_status);
+      return launch_check("masked copy");
+    }
+    w.elem_norm = nullptr;
+    w.V = bf.S2;
+    w.U0 = bf.S0;
+    w.out = bf.S1;
+    w.stage = 2;
+    w.a = 0.75;
+    w.b = 0.25;
+    if (dispatch(m, B.phys[b], w, st)) return -1;
+    w.V = bf.S1;
+    w.out = bf.S0;
+    w.stage = 3;
+    w.a = 1.0 / 3.0;
+    w.b = 2.0 / 3.0;
+    if (dispatch(m, B.phys[b], w, st)) return -1;
+  }
+  return 0;
+}
+
+static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
+  const int key = 2 * n + (first ? 1 : 0);
+  auto it = B.graphs.find(key);
+  if (it != B.graphs.end()) {
+    *out = it->second;
+    return 0;
+  }
+  cudaGraph_t g = nullptr;
+  if (cuda_check(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return -1;
+  // fork: every bucket's n steps on its own stream, then join before the check
+  int rc = cuda_check(cudaEventRecord(B.fork, B.stream), "fork record");
+  for (size_t b = 0; b < B.mesh.size() && rc == 0; ++b) {
+    rc = cuda_check(cudaStreamWaitEvent(B.bstream[b], B.fork, 0), "fork wait");
+    for (int i = 0; i < n && rc == 0; ++i) rc = enqueue_bucket_step(B, b, B.bstream[b]);
+    if (rc == 0) rc = cuda_check(cudaEventRecord(B.bdone[b], B.bstream[b]), "join record");
+    if (rc == 0) rc = cuda_check(cudaStreamWaitEvent(B.stream, B.bdone[b], 0), "join wait");
+  }
+  if (rc == 0) rc = cuda_check(cudaMemsetAsync(B.bm.n_running, 0, sizeof(int32_t), B.stream), "memset");
+  if (rc == 0) {
+    k_batch_check<<<(unsigned)B.bm.n_inst, 256, 0, B.stream>>>(B.bm, n, first);
+    rc = launch_check("batch check");
+  }
+  const cudaError_t end = cudaStreamEndCapture(B.stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return -1;
+  }
+  if (cuda_check(end, "end capture")) return -1;
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t inst = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (cuda_check(inst, "graph instantiate")) return -1;
+  B.graphs[key] = ex;
+  *out = ex;
+  return 0;
+}
+
 }  // namespace nzb
 
 using namespace nzb;
@@ -376,6 +534,7 @@ int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_arg
   w.out = a->out;
   w.dt = a->dt;
   w.norm_partial = a->norm_partial;
+  w.elem_norm = a->elem_norm;
   w.counters = a->counters;
   w.flags = a->flags;
   w.dt_factor = a->dt_factor;
@@ -452,6 +611,95 @@ int nzb_solver_run(nzb_solver* solver, int n_steps, void* stream) {
   if (cuda_check(cudaEventRecord(s->ev_out, s->stream), "event record") ||
       cuda_check(cudaStreamWaitEvent(caller, s->ev_out, 0), "stream wait"))
     return -1;
+  return 0;
+}
+
+int nzb_batch_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics* phys, const nzb_buffers* buffers,
+                     const int64_t* elem_offset, const double* dt_factor, const nzb_batch_march* march,
+                     nzb_batch** out) {
+  if (!out) return fail("batch_create: out is null");
+  *out = nullptr;
+  if (n_buckets < 1 || !meshes || !phys || !buffers || !elem_offset || !dt_factor || !march)
+    return fail("batch_create: null argument");
+  const nzb_batch_march& bm = *march;
+  if (bm.n_inst < 1 || !bm.inst_begin || !bm.inst_end || !bm.inst_count || !bm.inst_tol || !bm.elem_norm ||
+      !bm.status || !bm.iterations || !bm.res0 || !bm.res || !bm.window || !bm.window_count || !bm.n_running)
+    return fail("batch_create: missing march array");
+  if (bm.stall_window < 2 || bm.max_iterations < 1) return fail("batch_create: bad march parameters");
+  if (bm.n_inst > 0x7fffffff) return fail("batch_create: too many instances");
+  Batch* B = new Batch();
+  for (int b = 0; b < n_buckets; ++b) {
+    if (check_mesh(&meshes[b])) {
+      delete B;
+      return -1;
+    }
+    if (!meshes[b].elem_inst || !meshes[b].inst_status) {
+      delete B;
+      return fail("batch_create: bucket meshes need elem_inst and inst_status");
+    }
+    const nzb_buffers& bf = buffers[b];
+    if (!bf.S0 || !bf.S1 || !bf.dt || (meshes[b].order > 0 && !bf.S2)) {
+      delete B;
+      return fail("batch_create: missing bucket buffer");
+    }
+    B->mesh.push_back(meshes[b]);
+    B->phys.push_back(phys[b]);
+    B->buf.push_back(bf);
+    B->offset.push_back(elem_offset[b]);
+    B->factor.push_back(dt_factor[b]);
+  }
+  B->bm = bm;
+  if (cuda_check(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking), "batch stream") ||
+      cuda_check(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming), "batch event") ||
+      cuda_check(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming), "batch event") ||
+      cuda_check(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming), "batch event")) {
+    nzb_batch_destroy(reinterpret_cast<nzb_batch*>(B));
+    return -1;
+  }
+  for (int b = 0; b < n_buckets; ++b) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    const int rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "bucket stream") ||
+                   cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "bucket event");
+    if (s) B->bstream.push_back(s);
+    if (ev) B->bdone.push_back(ev);
+    if (rc) {
+      nzb_batch_destroy(reinterpret_cast<nzb_batch*>(B));
+      return -1;
+    }
+  }
+  *out = reinterpret_cast<nzb_batch*>(B);
+  return 0;
+}
+
+int nzb_batch_run(nzb_batch* batch, int n_steps, int first, void* stream) {
+  Batch* B = reinterpret_cast<Batch*>(batch);
+  if (!B) return fail("batch is null");
+  if (n_steps < 1 || (first && n_steps != 1)) return fail("batch_run: n_steps >= 1, and 1 for the first chunk");
+  cudaStream_t caller = (cudaStream_t)stream;
+  if (cuda_check(cudaEventRecord(B->ev_in, caller), "event record") ||
+      cuda_check(cudaStreamWaitEvent(B->stream, B->ev_in, 0), "stream wait"))
+    return -1;
+  cudaGraphExec_t ex = nullptr;
+  if (batch_graph(*B, n_steps, first, &ex)) return -1;
+  if (cuda_check(cudaGraphLaunch(ex, B->stream), "graph launch")) return -1;
+  if (cuda_check(cudaEventRecord(B->ev_out, B->stream), "event record") ||
+      cuda_check(cudaStreamWaitEvent(caller, B->ev_out, 0), "stream wait"))
+    return -1;
+  return 0;
+}
+
+int nzb_batch_destroy(nzb_batch* batch) {
+  Batch* B = reinterpret_cast<Batch*>(batch);
+  if (!B) return 0;
+  for (auto& kv : B->graphs) cudaGraphExecDestroy(kv.second);
+  if (B->ev_in) cudaEventDestroy(B->ev_in);
+  if (B->ev_out) cudaEventDestroy(B->ev_out);
+  if (B->fork) cudaEventDestroy(B->fork);
+  for (auto ev : B->bdone) cudaEventDestroy(ev);
+  for (auto s : B->bstream) cudaStreamDestroy(s);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
   return 0;
 }
 

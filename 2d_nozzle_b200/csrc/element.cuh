@@ -2,22 +2,28 @@
 // inverse mass, stage update and positivity limiter in one pass per element.
 //
 // One thread owns one element.  Its NP x 4 coefficients and NP x 4 residual
-// accumulators live in registers; every reference-element table is read from
-// constant memory at a compile-time address, so each multiply-add is a single
-// DFMA with a constant-bank operand.  The face integral is computed from the
-// element's own side: both traces are formed (the neighbour's from the p + 1
-// coefficients on the shared edge, read straight from HBM/L2), and the flux is
-// evaluated with the owner's trace as the left state and the owner's normal, so
-// the owner and the neighbour of an edge compute bit-identical fluxes and the
-// scheme stays conservative with no edge array and no second pass.
+// accumulators live in registers; the volume loops are fully unrolled, so each
+// reference-element table entry is a constant-bank operand at a compile-time
+// address and every multiply-add is a single DFMA with no load.  The face
+// integral is computed from the element's own side in a rolled loop (one copy
+// of the flux code): both traces are formed from the p + 1 coefficients on the
+// shared edge -- the neighbour's read straight from HBM/L2 -- and the flux is
+// evaluated with the owner's trace as the left state and the owner's normal,
+// so both elements of an edge compute bit-identical fluxes and the scheme stays
+// conservative with no edge array and no second pass.  The lift accumulates in
+// a per-thread column of shared memory.
 //
 // Mathematics (src/spatial/assembly.py:52-162, src/backends/_numba_kernels.py:
 // 484-777): R_i = -sum_q (gx_iq F_q + gy_iq G_q) + sum_f sign_f sum_q phi_f,iq fw_q
 // with fw = flux * |dX/dsigma| * w_q, the rate -M^-1 R, and
-// wave = sum_f max_q s_q * length_f.  For straight-sided triangles
-// gx = det * w_q (dphi/dxi xi_x + dphi/deta eta_x) and M = det * M_ref, so the
-// kernel carries five numbers per element instead of the reference's
-// per-element operator arrays.
+// wave = sum_f max_q s_q * length_f, where gx = w det (dphi/dxi xi_x +
+// dphi/deta eta_x).  Geometry comes in two layouts:
+//   affine  (straight-sided triangles): xi_x, xi_y, eta_x, eta_y, det per
+//           element; M = det M_ref, so M^-1 is a table divided by det;
+//   general (bilinear quadrilaterals, or any straight-sided element): the
+//           vertex coordinates, from which every volume point's Jacobian is
+//           rebuilt (det * (xi_x, xi_y) = (y_eta, -x_eta) needs no division),
+//           and the element's inverse mass matrix.
 #pragma once
 #include "physics.cuh"
 #include "shapes.cuh"
@@ -25,7 +31,6 @@
 namespace nzb {
 
 __constant__ double c_tab[TABLE_DOUBLES];
-
 
 enum { OP_RESIDUAL = 0, OP_RATE = 1, OP_STAGE = 2, OP_LIMIT = 3 };
 
@@ -37,6 +42,7 @@ struct Work {
   double* wave;
   double* dt;
   double* norm_partial;
+  double* elem_norm;  // per-element stage-1 norm contribution (batches)
   unsigned long long* counters;
   uint8_t* flags;
   double dt_factor, a, b;
@@ -48,12 +54,20 @@ __device__ __forceinline__ double tab(int idx) {
   return c_tab[idx];
 }
 
-// One probe point (volume point pt < NQV, else own face point) of this
-// element's solution: w = sum_i basis_i(pt) u_i.  pt is the same on every lane
-// of the warp (the loops over points are rolled and uniform), so the table
-// reads are constant-cache broadcasts and the kernel stays small.
+// Reference face basis phi_face[side, f, edge_node(f, j), q] (runtime indices).
 template <int K, int P>
-__device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4], int pt, double (&w)[4]) {
+__device__ __forceinline__ double pfe(int side, int f, int j, int q) {
+  using S = Shape<K, P>;
+  return c_tab[S::O_PFE + ((side * S::NF + f) * S::NE + j) * S::NQF + q];
+}
+
+// One probe point of this element's solution: volume point pt < NQV, else the
+// element's own trace at face point (f, q), with the basis of its side of that
+// face (bit f of sides), as the reference's probe set (src/spatial/limiter.py:
+// 78-95).  pt is the same on every lane of a warp (the loops over points are
+// rolled), so the table reads are constant-cache broadcasts.
+template <int K, int P>
+__device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4], int pt, int sides, double (&w)[4]) {
   using S = Shape<K, P>;
   w[0] = w[1] = w[2] = w[3] = 0.0;
   if (pt < S::NQV) {
@@ -65,21 +79,20 @@ __device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4
     }
   } else {
     const int f = (pt - S::NQV) / S::NQF, q = (pt - S::NQV) - f * S::NQF;
+    const int side = (sides >> f) & 1;
 #pragma unroll
     for (int j = 0; j < S::NE; ++j) {
-      const double l = c_tab[S::O_E1D + j * S::NQF + q];
-      const int n = edge_node(K, P, f, j);
-      // u is indexed at a runtime node: select it from the unrolled candidates
-      double v[4] = {u[0][0], u[0][1], u[0][2], u[0][3]};
+      const double l = pfe<K, P>(side, f, j, q);
+      // u at a runtime node: select among the unrolled candidates
+      double v[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int ff = 0; ff < S::NF; ++ff) {
-        const int nn = edge_node(K, P, ff, j);
         if (ff == f) {
+          const int nn = edge_node(K, P, ff, j);
 #pragma unroll
           for (int s = 0; s < 4; ++s) v[s] = u[nn][s];
         }
       }
-      (void)n;
 #pragma unroll
       for (int s = 0; s < 4; ++s) w[s] = fma(l, v[s], w[s]);
     }
@@ -91,17 +104,16 @@ __device__ __forceinline__ double pressure_at(const double (&w)[4], double g) {
   return (g - 1.0) * (w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / r);
 }
 
-// Minimum density and pressure over the limiter's probe set -- volume points
-// plus the element's own face points -- of ubar + theta (u - ubar), through the
+// Minimum pressure over the probe set of ubar + theta (u - ubar), through the
 // reference's scaling formula (src/spatial/limiter.py:146-148,151-178).
 template <int K, int P>
 __device__ __forceinline__ double pmin_at(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4], double theta,
-                                          double g) {
+                                          int sides, double g) {
   double pmin = 1e300;
 #pragma unroll 1
   for (int pt = 0; pt < Shape<K, P>::NPROBE; ++pt) {
     double w[4];
-    probe_point<K, P>(u, pt, w);
+    probe_point<K, P>(u, pt, sides, w);
 #pragma unroll
     for (int s = 0; s < 4; ++s) w[s] = ub[s] + theta * (w[s] - ub[s]);
     const double pp = pressure_at(w, g);
@@ -116,7 +128,7 @@ __device__ __forceinline__ double pmin_at(const double (&u)[Shape<K, P>::NP][4],
 // h(t) = rho(t) (p(t) - eps_p) / (gamma - 1) = a t^2 + b t + c with
 // h(0) = rho_bar (p_bar - eps_p) / (gamma - 1) > 0; t* = 1e300 when no point binds.
 template <int K, int P>
-__device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4],
+__device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4], int sides,
                                            double eps_p, double g, double& rmin, double& pmin, double& tstar) {
   const double e1 = eps_p / (g - 1.0);
   const double c = ub[3] * ub[0] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) - e1 * ub[0];
@@ -126,14 +138,14 @@ __device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4]
 #pragma unroll 1
   for (int pt = 0; pt < Shape<K, P>::NPROBE; ++pt) {
     double w[4];
-    probe_point<K, P>(u, pt, w);
+    probe_point<K, P>(u, pt, sides, w);
     rmin = w[0] < rmin ? w[0] : rmin;
     const double pp = pressure_at(w, g);
     pmin = pp < pmin ? pp : pmin;
     const double d0 = w[0] - ub[0], d1 = w[1] - ub[1], d2 = w[2] - ub[2], d3 = w[3] - ub[3];
     const double a = d3 * d0 - 0.5 * (d1 * d1 + d2 * d2);
     const double b = ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0;
-    // h > 0 for every t > 0 when it starts increasing and curves up
+    // h stays positive for t > 0 when it starts increasing and curves up
     if (a >= 0.0 && b >= 0.0) continue;
     const double disc = b * b - 4.0 * a * c;
     if (disc < 0.0) continue;
@@ -145,18 +157,60 @@ __device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4]
   }
 }
 
+// Jacobian of the element map at volume point q (general geometry, Q = 1),
+// from the vertex coordinates: returns det = x_xi y_eta - x_eta y_xi.
+template <int K, int P>
+__device__ __forceinline__ double point_det(const double (&xv)[Shape<K, P>::NF], const double (&yv)[Shape<K, P>::NF],
+                                            int q, double& x_xi, double& x_eta, double& y_xi, double& y_eta) {
+  using S = Shape<K, P>;
+  x_xi = x_eta = y_xi = y_eta = 0.0;
+#pragma unroll
+  for (int v = 0; v < S::NF; ++v) {
+    const double dx = tab<K, P>(S::O_DGX + v * S::NQV + q), de = tab<K, P>(S::O_DGE + v * S::NQV + q);
+    x_xi = fma(dx, xv[v], x_xi);
+    x_eta = fma(de, xv[v], x_eta);
+    y_xi = fma(dx, yv[v], y_xi);
+    y_eta = fma(de, yv[v], y_eta);
+  }
+  return x_xi * y_eta - x_eta * y_xi;
+}
+
 // Zhang-Shu positivity limiter of one element, in place
 // (src/spatial/limiter.py:103-243; the O(NP) Lebesgue screen of
 // src/backends/_numba_kernels.py:1010-1026 skips provably admissible elements).
 template <int K, int P, bool AFF>
 __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], const nzb_mesh& m,
-                                              const nzb_physics& ph, int64_t e, int& scaled, int& repaired) {
+                                              const nzb_physics& ph, int64_t e, int sides, int& scaled,
+                                              int& repaired) {
   using S = Shape<K, P>;
   const double g = ph.gamma;
   const int64_t E = m.n_elem;
+  // cell-average weights: a table for affine elements (M = det M_ref), else
+  // sum_q phi_iq w_q det_q / area, as the reference builds them
   double mw[S::NP];
+  if (AFF) {
 #pragma unroll
-  for (int i = 0; i < S::NP; ++i) mw[i] = AFF ? tab<K, P>(S::O_MW + i) : __ldg(m.mean_w + i * E + e);
+    for (int i = 0; i < S::NP; ++i) mw[i] = tab<K, P>(S::O_MW + i);
+  } else {
+    double xv[S::NF], yv[S::NF];
+#pragma unroll
+    for (int v = 0; v < S::NF; ++v) {
+      xv[v] = __ldg(m.geo + v * E + e);
+      yv[v] = __ldg(m.geo + (S::NF + v) * E + e);
+    }
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i) mw[i] = 0.0;
+#pragma unroll
+    for (int q = 0; q < S::NQV; ++q) {
+      double a, b, c, d;
+      const double wdet = tab<K, P>(S::O_WV + q) * point_det<K, P>(xv, yv, q, a, b, c, d);
+#pragma unroll
+      for (int i = 0; i < S::NP; ++i) mw[i] = fma(tab<K, P>(S::O_PHI + i * S::NQV + q), wdet, mw[i]);
+    }
+    const double area = __ldg(m.area + e);
+#pragma unroll
+    for (int i = 0; i < S::NP; ++i) mw[i] = mw[i] / area;
+  }
   double ub[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int i = 0; i < S::NP; ++i)
@@ -202,7 +256,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
     if (p_lo >= eps_p) return;
   }
   double rmin, pmin, tstar;
-  probe_scan<K, P>(u, ub, eps_p, g, rmin, pmin, tstar);
+  probe_scan<K, P>(u, ub, sides, eps_p, g, rmin, pmin, tstar);
   if (!(rmin < eps_r) && !(pmin < eps_p)) return;
 
   double theta = 1.0;
@@ -221,7 +275,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
   // the reference's pointwise arithmetic -- is taken with that arithmetic.
   auto admissible = [&](double t) -> bool {
     if (fabs(t - tstar) > 1e-7 * theta) return t < tstar;
-    return pmin_at<K, P>(u, ub, t, g) >= eps_p;
+    return pmin_at<K, P>(u, ub, t, sides, g) >= eps_p;
   };
   if (!admissible(theta)) {
     double lo = 0.0, hi = theta;
@@ -251,7 +305,7 @@ __device__ __forceinline__ void block_sum_store(double v, double* dst) {
   if (threadIdx.x == 0) {
     double t = 0.0;
 #pragma unroll
-    for (int w = 0; w < NW; ++w) t += red[w];
+    for (int k = 0; k < NW; ++k) t += red[k];
     *dst = t;
   }
 }
@@ -263,6 +317,15 @@ struct Launch {
   static constexpr int NP = Shape<K, P>::NP;
   static constexpr int NT = (NP * 4 * 8 * 128 <= 40 * 1024) ? 128 : 64;
 };
+
+// Face bits of this element (bit f = its side of face f) from the mesh arrays.
+template <int K, int P>
+__device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
+  int sides = 0;
+#pragma unroll
+  for (int f = 0; f < Shape<K, P>::NF; ++f) sides |= (__ldg(m.face_code + f * m.n_elem + e) & 1) << f;
+  return sides;
+}
 
 // LIM = false compiles the residual / rate variant, without the stage update
 // and the limiter (a smaller kernel: fewer registers, no instruction-cache
@@ -277,7 +340,11 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
   const int t = threadIdx.x;
   const int64_t E = m.n_elem;
   const int64_t e = (int64_t)blockIdx.x * BT + t;
-  const bool active = e < E;
+  // a retired instance of a batch is left untouched
+  int inst = -1;
+  if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
+  const bool active = e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0);
+  const double p_back = (inst >= 0 && m.inst_p_back) ? __ldg(m.inst_p_back + inst) : ph.p_back;
   const double g = ph.gamma;
   double nrm = 0.0;
   int scaled = 0, repaired = 0;
@@ -288,7 +355,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
     for (int i = 0; i < NP; ++i)
 #pragma unroll
       for (int s = 0; s < 4; ++s) u[i][s] = w.V[(s * NP + i) * E + e];
-    if (LIM && ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
+    if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, face_sides<K, P>(m, e), scaled, repaired);
 #pragma unroll
     for (int i = 0; i < NP; ++i)
 #pragma unroll
@@ -297,89 +364,79 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
   } else if (active) {
     const bool rate = w.op != OP_RESIDUAL;
     double xx = 0, xy = 0, yx = 0, yy = 0, det = 1.0;
+    double xv[NF], yv[NF];
     if (AFF) {
       xx = __ldg(m.geo + 0 * E + e);
       xy = __ldg(m.geo + 1 * E + e);
       yx = __ldg(m.geo + 2 * E + e);
       yy = __ldg(m.geo + 3 * E + e);
       det = __ldg(m.geo + 4 * E + e);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NF; ++v) {
+        xv[v] = __ldg(m.geo + v * E + e);
+        yv[v] = __ldg(m.geo + (NF + v) * E + e);
+      }
     }
 #pragma unroll
     for (int i = 0; i < NP * 4; ++i) facc[i * BT + t] = 0.0;
 
     // ---- face terms: a rolled loop over (face, point), so the flux code is
-    // inlined once.  The element's own and its neighbour's edge coefficients
-    // are read from HBM/L2; the lift goes to the shared-memory column.
+    // inlined once.  Traces use the reference's face basis phi_face[side, f] at
+    // the p + 1 edge nodes; the lift goes to the shared-memory column.
     const double fs = (AFF && rate) ? -1.0 / det : 1.0;
     double wave = 0.0;
+    int sides = 0;
 #pragma unroll 1
     for (int f = 0; f < NF; ++f) {
       const int code = __ldg(m.face_code + f * E + e);
       const int k = __ldg(m.face_edge + f * E + e);
       const int nb = __ldg(m.face_nbr + f * E + e);
-      const bool side = code & 1;
+      const int side = code & 1;
       const int nf = (code >> 1) & 7;
       const int tag = code >> 4;
+      sides |= side << f;
       const double nx = __ldg(m.edge_geo + 4 * (int64_t)k + 0);
       const double ny = __ldg(m.edge_geo + 4 * (int64_t)k + 1);
       const double jac = __ldg(m.edge_geo + 4 * (int64_t)k + 2);
       const double len = __ldg(m.edge_geo + 4 * (int64_t)k + 3);
       double ue[NE][4], un[NE][4];
       int node[NE];
-      if (AFF) {
+#pragma unroll
+      for (int j = 0; j < NE; ++j) {
+        node[j] = edge_node(K, P, f, j);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) ue[j][s] = __ldg(w.V + (s * NP + node[j]) * E + e);
+      }
+      if (nb >= 0) {
 #pragma unroll
         for (int j = 0; j < NE; ++j) {
-          node[j] = edge_node(K, P, f, j);
+          const int n = edge_node(K, P, nf, j);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) ue[j][s] = __ldg(w.V + (s * NP + node[j]) * E + e);
-        }
-        if (nb >= 0) {
-          // the neighbour's edge coefficients in the edge's (owner's) orientation
-#pragma unroll
-          for (int j = 0; j < NE; ++j) {
-            const int n = edge_node(K, P, nf, side ? j : NE - 1 - j);
-#pragma unroll
-            for (int s = 0; s < 4; ++s) un[j][s] = __ldg(w.V + (s * NP + n) * E + nb);
-          }
+          for (int s = 0; s < 4; ++s) un[j][s] = __ldg(w.V + (s * NP + n) * E + nb);
         }
       }
       const double coef = (side ? -1.0 : 1.0) * fs;
       double smax = 0.0;
 #pragma unroll 1
       for (int q = 0; q < NQF; ++q) {
-        double tc[4] = {0.0, 0.0, 0.0, 0.0}, tn[4] = {0.0, 0.0, 0.0, 0.0};
-        double cj[NE];
-        // general geometry: the reference's full face basis phi_face[side, f]
-        const int own = S::O_PF + ((side * NF + f) * NP) * NQF + q;
-        if (AFF) {
-          // side 1 walks the edge backwards: l_j(1 - sigma_q) = l_{p-j}(sigma_q)
+        // canonical (owner's) point q: own trace with phi_face[side, f],
+        // the neighbour's with phi_face[1 - side, nf]
+        double tc[4] = {0.0, 0.0, 0.0, 0.0}, tn[4] = {0.0, 0.0, 0.0, 0.0}, cj[NE];
 #pragma unroll
-          for (int j = 0; j < NE; ++j) {
-            const double l = c_tab[S::O_E1D + j * NQF + q];
-            const double r = c_tab[S::O_E1D + (NE - 1 - j) * NQF + q];
-            cj[j] = side ? r : l;
+        for (int j = 0; j < NE; ++j) {
+          cj[j] = pfe<K, P>(side, f, j, q);
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-              tc[s] = fma(cj[j], ue[j][s], tc[s]);
-              if (nb >= 0) tn[s] = fma(l, un[j][s], tn[s]);
-            }
-          }
-        } else {
-          const int oth = S::O_PF + (((1 - side) * NF + nf) * NP) * NQF + q;
-#pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            const double b = c_tab[own + i * NQF];
-#pragma unroll
-            for (int s = 0; s < 4; ++s) tc[s] = fma(b, __ldg(w.V + (s * NP + i) * E + e), tc[s]);
-            if (nb >= 0) {
-              const double bn = c_tab[oth + i * NQF];
-#pragma unroll
-              for (int s = 0; s < 4; ++s) tn[s] = fma(bn, __ldg(w.V + (s * NP + i) * E + nb), tn[s]);
-            }
-          }
+          for (int s = 0; s < 4; ++s) tc[s] = fma(cj[j], ue[j][s], tc[s]);
         }
         double F[4], sp;
         if (nb >= 0) {
+#pragma unroll
+          for (int j = 0; j < NE; ++j) {
+            const double l = pfe<K, P>(1 - side, nf, j, q);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) tn[s] = fma(l, un[j][s], tn[s]);
+          }
           double L[4], R[4];
 #pragma unroll
           for (int s = 0; s < 4; ++s) {
@@ -388,32 +445,20 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
           }
           sp = interface_flux(L, R, nx, ny, ph, F);
         } else {
-          sp = boundary_flux(tag, tc, nx, ny, ph, F);
+          sp = boundary_flux(tag, tc, nx, ny, ph, p_back, F);
         }
         smax = sp > smax ? sp : smax;
         const double scale = jac * c_tab[S::O_WF + q];
         double fwc[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) fwc[s] = (F[s] * scale) * coef;
-        if (AFF) {
 #pragma unroll
-          for (int j = 0; j < NE; ++j)
+        for (int j = 0; j < NE; ++j)
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-              double& a = facc[(node[j] * 4 + s) * BT + t];
-              a = fma(cj[j], fwc[s], a);
-            }
-        } else {
-#pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            const double b = c_tab[own + i * NQF];
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-              double& a = facc[(i * 4 + s) * BT + t];
-              a = fma(b, fwc[s], a);
-            }
+          for (int s = 0; s < 4; ++s) {
+            double& a = facc[(node[j] * 4 + s) * BT + t];
+            a = fma(cj[j], fwc[s], a);
           }
-        }
       }
       wave += smax * len;
     }
@@ -430,7 +475,9 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
           u[i][s] = __ldg(w.V + (s * NP + i) * E + e);
           acc[i][s] = facc[(i * 4 + s) * BT + t];
         }
-      const double vs = (AFF && !rate) ? -det : 1.0;
+      // affine: (xi_x F + xi_y G) det, det only for the residual (the rate
+      // divides it out again); general: det (xi_x, xi_y) = (y_eta, -x_eta)
+      const double vs = AFF ? (rate ? 1.0 : -det) : -1.0;
 #pragma unroll
       for (int q = 0; q < NQV; ++q) {
         double uq[4] = {0.0, 0.0, 0.0, 0.0};
@@ -443,28 +490,27 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
         const Prim pr = primitives_fast(uq, g);
         const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
         const double G[4] = {pr.rho * pr.vy, pr.rho * pr.vx * pr.vy, pr.rho * pr.vy * pr.vy + pr.p, pr.rho * pr.vy * pr.H};
-        if (AFF) {
-          double fx[4], fe[4];
+        double a00 = xx, a01 = xy, a10 = yx, a11 = yy;
+        if (!AFF) {
+          double x_xi, x_eta, y_xi, y_eta;
+          point_det<K, P>(xv, yv, q, x_xi, x_eta, y_xi, y_eta);
+          a00 = y_eta;
+          a01 = -x_eta;
+          a10 = -y_xi;
+          a11 = x_xi;
+        }
+        double fx[4], fe[4];
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            fx[s] = (xx * F[s] + xy * G[s]) * vs;
-            fe[s] = (yx * F[s] + yy * G[s]) * vs;
-          }
+        for (int s = 0; s < 4; ++s) {
+          fx[s] = (a00 * F[s] + a01 * G[s]) * vs;
+          fe[s] = (a10 * F[s] + a11 * G[s]) * vs;
+        }
 #pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            const double a = tab<K, P>(S::O_WXI + i * NQV + q);
-            const double b = tab<K, P>(S::O_WETA + i * NQV + q);
+        for (int i = 0; i < NP; ++i) {
+          const double a = tab<K, P>(S::O_WXI + i * NQV + q);
+          const double b = tab<K, P>(S::O_WETA + i * NQV + q);
 #pragma unroll
-            for (int s = 0; s < 4; ++s) acc[i][s] = fma(a, fx[s], fma(b, fe[s], acc[i][s]));
-          }
-        } else {
-#pragma unroll
-          for (int i = 0; i < NP; ++i) {
-            const double gx = __ldg(m.gx + (i * NQV + q) * E + e);
-            const double gy = __ldg(m.gy + (i * NQV + q) * E + e);
-#pragma unroll
-            for (int s = 0; s < 4; ++s) acc[i][s] -= gx * F[s] + gy * G[s];
-          }
+          for (int s = 0; s < 4; ++s) acc[i][s] = fma(a, fx[s], fma(b, fe[s], acc[i][s]));
         }
       }
     }
@@ -517,7 +563,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
         }
       }
       if (LIM && w.op == OP_STAGE) {
-        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, scaled, repaired);
+        if (w.elem_norm && w.stage == 1) w.elem_norm[e] = nrm;
+        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, sides, scaled, repaired);
 #pragma unroll
         for (int i = 0; i < NP; ++i)
 #pragma unroll
@@ -527,7 +574,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, 
     }
   }
   // block-level reductions (every thread of the block reaches these)
-  if (LIM && w.op == OP_STAGE && w.norm_partial && w.stage == 1) block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
+  if (LIM && w.op == OP_STAGE && w.norm_partial && w.stage == 1)
+    block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
   if (LIM && (w.op == OP_STAGE || w.op == OP_LIMIT) && w.counters) {
     const int ns = __syncthreads_count(scaled);
     const int nr = __syncthreads_count(repaired);

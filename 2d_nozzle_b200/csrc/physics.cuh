@@ -232,7 +232,7 @@ __device__ __forceinline__ double inflow_flux(const double* U, double nx, double
 }
 
 __device__ __forceinline__ double outflow_flux(const double* U, double nx, double ny, const nzb_physics& ph,
-                                               double* F) {
+                                               double p_back, double* F) {
   const double g = ph.gamma;
   const Prim s = primitives(U, g);
   const double a = sqrt(g * s.p / s.rho);
@@ -241,7 +241,7 @@ __device__ __forceinline__ double outflow_flux(const double* U, double nx, doubl
   if (vn / a >= 1.0) {
     Ub[0] = U[0]; Ub[1] = U[1]; Ub[2] = U[2]; Ub[3] = U[3];
   } else {
-    const double pb = ph.p_back;
+    const double pb = p_back;
     const double rhob = s.rho * pow(pb / s.p, 1.0 / g);
     const double ab = sqrt(g * pb / rhob);
     const double vnb = vn + 2.0 / (g - 1.0) * (a - ab);
@@ -275,9 +275,9 @@ __device__ __forceinline__ double interface_flux(const double* UL, const double*
 }
 
 __device__ __forceinline__ double boundary_flux(int tag, const double* U, double nx, double ny,
-                                                const nzb_physics& ph, double* F) {
+                                                const nzb_physics& ph, double p_back, double* F) {
   if (tag == NZB_INFLOW) return inflow_flux(U, nx, ny, ph, F);
-  if (tag == NZB_OUTFLOW) return outflow_flux(U, nx, ny, ph, F);
+  if (tag == NZB_OUTFLOW) return outflow_flux(U, nx, ny, ph, p_back, F);
   return wall_flux(U, nx, ny, ph.gamma, F);
 }
 

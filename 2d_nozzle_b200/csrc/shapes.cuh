@@ -29,11 +29,15 @@ __host__ __device__ constexpr int n_edge_nodes(int p) { return p + 1; }
 //   E1D [NE][NQF]   1D Lagrange basis of the edge nodes at the edge Gauss points
 //   WF  [NQF]       edge Gauss weights
 //   MW  [NP]        cell-average weights sum_q phi_i w_q / sum_q w_q
-//   PF  [2][NF][NP][NQF]  the reference's face basis phi_face[side, f, i, q]
+//   WV  [NQV]       volume weights
+//   DGX [NV][NQV]   d(vertex shape function)/dxi at the volume points (NV = NF)
+//   DGE [NV][NQV]   d(vertex shape function)/deta
+//   PFE [2][NF][NE][NQF]  the reference's face basis phi_face[side, f, i, q]
+//                   at the edge nodes i = edge_node(f, j)
 __host__ __device__ constexpr int slot_size(int kind, int p) {
   return 3 * n_basis(kind, p) * n_qvol(kind, p) + n_basis(kind, p) * n_basis(kind, p) +
-         n_edge_nodes(p) * n_qface(kind, p) + n_qface(kind, p) + n_basis(kind, p) +
-         2 * n_faces(kind) * n_basis(kind, p) * n_qface(kind, p);
+         n_edge_nodes(p) * n_qface(kind, p) + n_qface(kind, p) + n_basis(kind, p) + n_qvol(kind, p) +
+         2 * n_faces(kind) * n_qvol(kind, p) + 2 * n_faces(kind) * n_edge_nodes(p) * n_qface(kind, p);
 }
 __host__ __device__ constexpr int slot_offset(int kind, int p) {
   int off = 0;
@@ -61,7 +65,10 @@ struct Shape {
   static constexpr int O_E1D = O_MINV + NP * NP;
   static constexpr int O_WF = O_E1D + NE * NQF;
   static constexpr int O_MW = O_WF + NQF;
-  static constexpr int O_PF = O_MW + NP;
+  static constexpr int O_WV = O_MW + NP;
+  static constexpr int O_DGX = O_WV + NQV;
+  static constexpr int O_DGE = O_DGX + NF * NQV;
+  static constexpr int O_PFE = O_DGE + NF * NQV;
   static constexpr int NPROBE = NQV + NF * NQF;  // limiter probe points
 };
 

@@ -10,9 +10,10 @@ Two geometry layouts:
 * affine -- straight-sided triangles: ``(5, E)`` = xi_x, xi_y, eta_x, eta_y,
   det per element (40 B), the volume and mass operators coming from the
   constant tables because ``M_e = det_e M_ref`` exactly;
-* general -- any element (bilinear quadrilaterals): the reference's
-  per-element weighted gradients ``grad_x``, ``grad_y`` and inverse mass
-  matrices, stored index-major / element-minor so a warp reads them coalesced.
+* general -- any straight-sided element (bilinear quadrilaterals): the vertex
+  coordinates (the kernels rebuild the Jacobian at every volume point) and the
+  reference's per-element inverse mass matrices, index-major / element-minor so
+  a warp reads them coalesced.
 """
 
 from __future__ import annotations
@@ -44,9 +45,16 @@ def element_tables(ref) -> np.ndarray:
     e1d = np.asarray(ref.phi_face)[0, f0][nodes, :]
     wf = np.asarray(ref.w_face)
     mw = (phi @ w) / w.sum()
+    nf = re.n_faces(kind)
+    # Q = 1 geometry: the vertex shape functions are the first-order Lagrange basis
+    dgx = np.asarray(ref.dgeom_dxi_vol)
+    dge = np.asarray(ref.dgeom_deta_vol)
+    if dgx.shape[0] != nf:
+        raise NotImplementedError("device tables take straight-sided (Q=1) geometry")
     pf = np.asarray(ref.phi_face)  # (2, NF, NP, NQF)
+    pfe = np.stack([np.stack([pf[sd, f][re.edge_node_ids(kind, p, f), :] for f in range(nf)]) for sd in range(2)])
     return np.ascontiguousarray(np.concatenate([phi.ravel(), wxi.ravel(), weta.ravel(), minv.ravel(), e1d.ravel(), wf, mw,
-                                                pf.ravel()]))
+                                                w, dgx.ravel(), dge.ravel(), pfe.ravel()]))
 
 
 def lebesgue_constant(ref) -> float:
@@ -101,81 +109,109 @@ def physics_struct(flow, opts, ref) -> capi.Physics:
     return ph
 
 
-class DeviceMesh:
-    """Device-resident geometry and connectivity of one mesh."""
+def host_arrays(ops, *, force_general: bool = False) -> dict:
+    """The per-element / per-edge arrays of one mesh, in device (structure-of-arrays) layout."""
+    ref = ops.ref
+    if ref.kind not in KIND_IDS or not 0 <= ref.order <= MAX_ORDER:
+        raise NotImplementedError(f"device kernels cover tri/quad p=0..{MAX_ORDER}, not {ref.kind} p={ref.order}")
+    topo = ops.topology
+    if topo.geometry_order != 1:
+        raise NotImplementedError("device kernels take straight-sided (Q=1) elements")
+    E = int(ops.n_elem)
+    affine = is_affine(ops) and not force_general
+    out = {"affine": affine, "n_elem": E}
+    if affine:
+        out["geo"] = np.ascontiguousarray(affine_inverse_jacobian(ops).T)
+    else:
+        if getattr(ops, "inv_mass", None) is None:
+            raise ValueError("general geometry needs the inverse mass matrices (build_operators(..., lean=False))")
+        Xv = np.asarray(ops.node_coords)[np.asarray(topo.elem_nodes)]  # (E, NV, 2), Q = 1: the vertices
+        out["geo"] = np.ascontiguousarray(np.concatenate([Xv[:, :, 0].T, Xv[:, :, 1].T], axis=0))
+        out["minv"] = np.ascontiguousarray(np.asarray(ops.inv_mass).reshape(E, -1).T)
+    out["area"] = np.asarray(ops.elem_area, dtype=float)
+    ed = topo.edges
+    ni = ed.n_interior
+    fe = np.asarray(ed.face_edge)
+    side = np.asarray(ed.face_side)
+    interior = fe < ni
+    ke = np.where(interior, fe, 0)
+    other = np.where(side == 0, 1, 0)
+    nbr = np.where(interior, np.asarray(ed.iedge_elem)[ke, other], -1)
+    nbr_face = np.where(interior, np.asarray(ed.iedge_face)[ke, other], 0)
+    tag = np.where(interior, 0, np.asarray(ed.bedge_tag)[np.where(interior, 0, fe - ni)])
+    out["face_nbr"] = np.ascontiguousarray(nbr.T.astype(np.int32))
+    out["face_code"] = np.ascontiguousarray((side | (nbr_face << 1) | (tag << 4)).T.astype(np.int32))
+    out["face_edge"] = np.ascontiguousarray(fe.T.astype(np.int32))
+    nrm = np.asarray(ops.edge_normal)
+    jac = np.asarray(ops.edge_jac)
+    if np.abs(nrm - nrm[:, :1]).max() > 0.0 or np.abs(jac - jac[:, :1]).max() > 0.0:
+        raise NotImplementedError("device kernels take straight edges (one normal per edge)")
+    out["edge_geo"] = np.ascontiguousarray(np.stack([nrm[:, 0, 0], nrm[:, 0, 1], jac[:, 0], np.asarray(ops.edge_length)], axis=1))
+    return out
 
-    def __init__(self, ops, device=None, *, force_general: bool = False):
+
+def concat_arrays(parts: list[dict]) -> dict:
+    """Concatenate several meshes' arrays into one, offsetting the connectivity."""
+    out = {"affine": parts[0]["affine"], "n_elem": sum(p["n_elem"] for p in parts)}
+    e_off = np.cumsum([0] + [p["n_elem"] for p in parts])
+    k_off = np.cumsum([0] + [p["edge_geo"].shape[0] for p in parts])
+    for name in ("geo", "minv", "face_code"):
+        if name in parts[0]:
+            out[name] = np.ascontiguousarray(np.concatenate([p[name] for p in parts], axis=1))
+    out["area"] = np.concatenate([p["area"] for p in parts])
+    out["face_nbr"] = np.ascontiguousarray(np.concatenate(
+        [np.where(p["face_nbr"] >= 0, p["face_nbr"] + e_off[i], -1) for i, p in enumerate(parts)], axis=1).astype(np.int32))
+    out["face_edge"] = np.ascontiguousarray(np.concatenate([p["face_edge"] + k_off[i] for i, p in enumerate(parts)], axis=1)
+                                            .astype(np.int32))
+    out["edge_geo"] = np.ascontiguousarray(np.concatenate([p["edge_geo"] for p in parts], axis=0))
+    if out["n_elem"] >= 2**31 or out["edge_geo"].shape[0] >= 2**31:
+        raise ValueError("a bucket is limited to 2^31 elements and edges")
+    return out
+
+
+class DeviceMesh:
+    """Device-resident geometry and connectivity of one mesh (or one batch bucket)."""
+
+    def __init__(self, ops=None, device=None, *, force_general: bool = False, arrays: dict | None = None, ref=None):
         import torch
 
         self.torch = torch
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise capi.NativeError("the B200 backend runs on a CUDA device only")
-        ref = ops.ref
-        if ref.kind not in KIND_IDS or not 0 <= ref.order <= MAX_ORDER:
-            raise NotImplementedError(f"device kernels cover tri/quad p=0..{MAX_ORDER}, not {ref.kind} p={ref.order}")
-        topo = ops.topology
-        if topo.geometry_order != 1:
-            raise NotImplementedError("device kernels take straight-sided (Q=1) elements")
+        if arrays is None:
+            arrays = host_arrays(ops, force_general=force_general)
+            ref = ops.ref
         self.ref = ref
         self.kind, self.order = ref.kind, int(ref.order)
         self.np_ = int(ref.n_basis)
         self.nf = re.n_faces(ref.kind)
-        self.E = int(ops.n_elem)
-        self.affine = is_affine(ops) and not force_general
+        self.E = int(arrays["n_elem"])
+        self.affine = bool(arrays["affine"])
         idx = self.device.index if self.device.index is not None else torch.cuda.current_device()
         ensure_tables(ref, idx)
-
-        def dev(a, dtype=torch.float64):
-            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=self.device)
-
-        E = self.E
         keep = {}
-        if self.affine:
-            keep["geo"] = dev(affine_inverse_jacobian(ops).T)
-        else:
-            if getattr(ops, "grad_x", None) is None:
-                raise ValueError("general geometry needs the per-element operators (build_operators(..., lean=False))")
-            keep["gx"] = dev(np.asarray(ops.grad_x).reshape(E, -1).T)
-            keep["gy"] = dev(np.asarray(ops.grad_y).reshape(E, -1).T)
-            keep["minv"] = dev(np.asarray(ops.inv_mass).reshape(E, -1).T)
-            keep["mean_w"] = dev(np.asarray(ops.mean_weights).T)
-        keep["area"] = dev(np.asarray(ops.elem_area))
-
-        ed = topo.edges
-        ni = ed.n_interior
-        fe = np.asarray(ed.face_edge)
-        side = np.asarray(ed.face_side)
-        interior = fe < ni
-        ke = np.where(interior, fe, 0)
-        other = np.where(side == 0, 1, 0)
-        nbr = np.where(interior, np.asarray(ed.iedge_elem)[ke, other], -1)
-        nbr_face = np.where(interior, np.asarray(ed.iedge_face)[ke, other], 0)
-        tag = np.where(interior, 0, np.asarray(ed.bedge_tag)[np.where(interior, 0, fe - ni)])
-        code = side | (nbr_face << 1) | (tag << 4)
-        keep["face_nbr"] = dev(nbr.T, torch.int32)
-        keep["face_code"] = dev(code.T, torch.int32)
-        keep["face_edge"] = dev(fe.T, torch.int32)
-
-        nrm = np.asarray(ops.edge_normal)
-        jac = np.asarray(ops.edge_jac)
-        if np.abs(nrm - nrm[:, :1]).max() > 0.0 or np.abs(jac - jac[:, :1]).max() > 0.0:
-            raise NotImplementedError("device kernels take straight edges (one normal per edge)")
-        egeo = np.stack([nrm[:, 0, 0], nrm[:, 0, 1], jac[:, 0], np.asarray(ops.edge_length)], axis=1)
-        keep["edge_geo"] = dev(egeo)
-        self.n_edge = int(egeo.shape[0])
+        for name, a in arrays.items():
+            if isinstance(a, np.ndarray):
+                keep[name] = torch.as_tensor(a, device=self.device)
+        self.n_edge = int(arrays["edge_geo"].shape[0])
         self.arrays = keep
-
         m = capi.Mesh()
         m.kind = KIND_IDS[self.kind]
         m.order = self.order
         m.affine = 1 if self.affine else 0
-        m.n_elem = E
+        m.n_elem = self.E
         m.n_edge = self.n_edge
-        for name in ("geo", "gx", "gy", "minv", "mean_w", "area", "face_nbr", "face_code", "face_edge", "edge_geo"):
+        for name in ("geo", "minv", "area", "face_nbr", "face_code", "face_edge", "edge_geo"):
             setattr(m, name, keep[name].data_ptr() if name in keep else None)
         self.c = m
         self.c_ref = C.byref(m)
+
+    def set_batch(self, elem_inst, inst_status, inst_p_back) -> None:
+        """Attach the batch arrays (device tensors kept alive by the caller)."""
+        self.c.elem_inst = elem_inst.data_ptr()
+        self.c.inst_status = inst_status.data_ptr()
+        self.c.inst_p_back = inst_p_back.data_ptr() if inst_p_back is not None else None
 
     def state(self) -> object:
         """An uninitialised (4, NP, E) device state."""
@@ -200,4 +236,3 @@ class DeviceMesh:
         out = self.torch.empty((self.E, self.np_, 4), dtype=self.torch.float64, device=self.device)
         capi.check(capi.load().nzb_unpack_state(soa.data_ptr(), out.data_ptr(), self.E, self.np_, None, self.stream()), "nzb_unpack_state")
         return out
-

@@ -48,15 +48,21 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * affine = 1: straight-sided triangles; geo holds (5, E) = xi_x, xi_y, eta_x,
  *             eta_y, det and the volume / mass operators come from the
  *             reference-element tables uploaded by nzb_upload_tables.
- * affine = 0: any element; gx, gy hold (NP*NQV, E) weighted gradients
- *             w det dphi/dx (the reference's Operators.grad_x / grad_y),
- *             minv (NP*NP, E) the inverse mass matrices, mean_w (NP, E).
+ * affine = 0: any straight-sided element (bilinear quadrilaterals): geo holds
+ *             (2*NV, E) = the NV vertex x then y coordinates, from which the
+ *             kernels rebuild the Jacobian at every volume point; minv holds
+ *             (NP*NP, E) the inverse mass matrices.
  * face_nbr  (NF, E): element across face f, or -1 on a boundary.
  * face_code (NF, E): side (bit 0: 0 owner, 1 neighbour) | neighbour's local
  *             face << 1 | boundary tag << 4.
  * face_edge (NF, E): global edge id.
  * edge_geo  (n_edge, 4): nx, ny (owner's outward unit normal), |dX/dsigma|,
  *             edge length.  Edges are straight: one normal per edge.
+ * Batches of independent instances share one mesh descriptor: their elements
+ * are concatenated (connectivity offset accordingly) and
+ * elem_inst   (E)      instance of each element (null: a single instance),
+ * inst_status (n_inst) nonzero = retired: its elements are left untouched,
+ * inst_p_back (n_inst) back pressure of each instance (null: phys.p_back).
  */
 typedef struct {
   int32_t kind;
@@ -66,15 +72,15 @@ typedef struct {
   int64_t n_elem;
   int64_t n_edge;
   const double* geo;
-  const double* gx;
-  const double* gy;
   const double* minv;
-  const double* mean_w;
   const double* area;
   const int32_t* face_nbr;
   const int32_t* face_code;
   const int32_t* face_edge;
   const double* edge_geo;
+  const int32_t* elem_inst;
+  const int32_t* inst_status;
+  const double* inst_p_back;
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly
@@ -138,6 +144,7 @@ typedef struct {
   double* out;
   double* dt;
   double* norm_partial;
+  double* elem_norm; /* (E, nullable): per-element sum (w F)^2 of stage 1, for batches */
   unsigned long long* counters;
   uint8_t* flags;
   double dt_factor;
@@ -178,6 +185,46 @@ int nzb_solver_create(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_b
                       int scheme_ssprk3, double dt_factor, nzb_solver** out);
 int nzb_solver_run(nzb_solver* solver, int n_steps, void* stream);
 int nzb_solver_destroy(nzb_solver* solver);
+
+/* ---- batched steady march: many independent instances, one launch per stage
+ * and bucket.  Instances are grouped in buckets of one (kind, order); each
+ * bucket is an nzb_mesh over the concatenated elements of its instances, with
+ * elem_inst / inst_status / inst_p_back set.  The march bookkeeping of every
+ * instance (src/timestepping/march.py:125-230) runs on the device after each
+ * chunk: the residual of its last step's stage-1 rate, then convergence,
+ * non-finite, divergence, stall window and iteration cap; a retired instance
+ * stops being advanced.  A chunk of n steps is one CUDA graph. */
+typedef struct {
+  int64_t n_inst;
+  const int64_t* inst_begin;  /* (n_inst) first element, in the global element numbering */
+  const int64_t* inst_end;    /* (n_inst) one past the last element */
+  const double* inst_count;   /* (n_inst) 4 * NP * E_i, the norm's divisor */
+  const double* inst_tol;     /* (n_inst) tolerance * residual scale */
+  double* elem_norm;          /* (sum E) per-element norm contributions (scratch) */
+  int32_t* status;            /* (n_inst) 0 running, 1 converged, 2 non-finite, 3 diverged, 4 stalled, 5 max_iterations */
+  int32_t* iterations;        /* (n_inst) steps taken */
+  double* res0;               /* (n_inst) */
+  double* res;                /* (n_inst) residual at the last check */
+  double* window;             /* (n_inst * stall_window) */
+  int32_t* window_count;      /* (n_inst) */
+  int32_t* n_running;         /* (1) */
+  double divergence_factor;
+  double stall_ratio;
+  int32_t stall_window;
+  int32_t max_iterations;
+} nzb_batch_march;
+typedef struct nzb_batch nzb_batch;
+/* buckets: n_buckets meshes (device pointers inside), their physics and
+ * buffers (S0, S1, S2, dt used; res / norm_partial / counters ignored),
+ * elem_offset[b] = the bucket's first element in the global numbering,
+ * dt_factor[b]. */
+int nzb_batch_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics* phys, const nzb_buffers* buffers,
+                     const int64_t* elem_offset, const double* dt_factor, const nzb_batch_march* march,
+                     nzb_batch** out);
+/* Advance every running instance by n_steps (first = 1 for the initial
+ * single step that sets res0), then run the device check. */
+int nzb_batch_run(nzb_batch* batch, int n_steps, int first, void* stream);
+int nzb_batch_destroy(nzb_batch* batch);
 
 const char* nzb_last_error(void);
 int nzb_version(void);

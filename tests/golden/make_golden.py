@@ -235,10 +235,41 @@ def config3(n_steps=5):
           limited=np.stack(masks), n_steps=np.int64(n_steps))
 
 
+BATCH_CASES = [  # element, order, refine, area ratio, back pressure, contour
+    ("tri", 1, 0, 2.5, 0.15, "smooth"),
+    ("quad", 1, 0, 3.0, 0.995, "bell"),
+    ("tri", 2, 0, 1.8, 0.30, "conical"),
+    ("tri", 1, 1, 2.2, 0.10, "bell"),
+    ("quad", 2, 0, 2.5, 0.15, "bell"),
+]
+
+
+def batch_cases():
+    """Outcomes of a few HLLC solves at tolerance 1e-8 (Numba backend)."""
+    import json
+
+    from src.api import solve_nozzle
+    from src.post.postprocess import performance
+
+    out = []
+    for el, p, r, ar, pb, contour in BATCH_CASES:
+        res = solve_nozzle(element=el, order=p, refine=r, area_ratio=ar, back_pressure_ratio=pb, contour=contour,
+                           flux="hllc", tolerance=1e-8, max_iterations=6000, backend="numba", verbose=False)
+        row = {"case": [el, p, r, ar, pb, contour], "converged": bool(res.converged), "iterations": int(res.iterations),
+               "residual": float(res.residual), "message": res.message}
+        if res.converged:
+            perf = performance(res)
+            row.update(thrust=perf.thrust, mass_flow_in=perf.mass_flow_in, exit_mach=perf.exit_mach_area_averaged)
+        out.append(row)
+    with open(os.path.join(HERE, "batch_cases.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote batch_cases.json")
+
+
 if __name__ == "__main__":
     import src  # noqa: F401  -- fails loudly when the reference is not on PYTHONPATH
 
-    which = sys.argv[1:] or ["small", "rect", "config1", "config3"]
+    which = sys.argv[1:] or ["small", "rect", "config1", "config3", "batch"]
     if "small" in which:
         small_cases()
     if "rect" in which:
@@ -247,3 +278,5 @@ if __name__ == "__main__":
         config1()
     if "config3" in which:
         config3()
+    if "batch" in which:
+        batch_cases()
