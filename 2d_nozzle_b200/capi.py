@@ -133,6 +133,7 @@ SIGNATURES = [
     ("nzb_element_blocks", I64, [C.POINTER(Mesh)]),
     ("nzb_norm_finalize", C.c_int, [P, I64, C.c_double, P, P]),
     ("nzb_norm", C.c_int, [P, I64, C.c_int, P, P, P, P]),
+    ("nzb_norm_noalloc", C.c_int, [P, I64, C.c_int, P, P, P]),
     ("nzb_solver_create", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(Buffers), C.c_int, C.c_double, C.POINTER(P)]),
     ("nzb_solver_run", C.c_int, [P, C.c_int, P]),
     ("nzb_solver_destroy", C.c_int, [P]),

@@ -432,6 +432,36 @@ static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
   return 0;
 }
 
+// ---- the norm without caller-provided scratch ------------------------------------
+// Partial sums of nzb_norm_noalloc live in this file-scope array: one slot per
+// block of the partial-sum kernel, 128 elements per block.  Every GPU that
+// loads the library holds it (512 KiB) until the process exits.
+constexpr int64_t NOALLOC_MAX_BLOCKS = 65536;
+constexpr int64_t NOALLOC_MAX_ELEMENTS = NOALLOC_MAX_BLOCKS * NT;
+static __device__ __align__(256) double g_norm_scratch[NOALLOC_MAX_BLOCKS];
+
+static std::mutex g_scratch_mu;
+static std::map<int, double*> g_scratch_addr;  // device -> g_norm_scratch there
+
+// The device address of g_norm_scratch on the current device, looked up once
+// per device with that device current.  In host code the symbol itself is only
+// a host-side stand-in, never a device address.
+static int scratch_address(double** out) {
+  int dev = -1;
+  if (cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return -1;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  auto it = g_scratch_addr.find(dev);
+  if (it != g_scratch_addr.end()) {
+    *out = it->second;
+    return 0;
+  }
+  double* p = nullptr;
+  if (cuda_check(cudaGetSymbolAddress((void**)&p, g_norm_scratch), "cudaGetSymbolAddress(norm scratch)")) return -1;
+  g_scratch_addr[dev] = p;
+  *out = p;
+  return 0;
+}
+
 }  // namespace nzb
 
 using namespace nzb;
@@ -560,6 +590,20 @@ int nzb_norm(const double* A, int64_t E, int np, const double* w4, double* parti
   k_norm_partial<<<(unsigned)nb, NT, 0, (cudaStream_t)stream>>>(A, E, np, w4[0], w4[1], w4[2], w4[3], partial);
   if (launch_check("norm launch")) return -1;
   return nzb_norm_finalize(partial, nb, 4.0 * (double)E * np, out, stream);
+}
+
+int nzb_norm_noalloc(const double* A, int64_t E, int np, const double* w4, double* out, void* stream) {
+  if (!A || !w4 || !out || E <= 0 || np <= 0) return fail("norm_noalloc: bad arguments");
+  if (E > NOALLOC_MAX_ELEMENTS)
+    return fail("norm_noalloc: n_elem = " + std::to_string(E) + " exceeds its fixed scratch, which holds " +
+                std::to_string(NOALLOC_MAX_ELEMENTS) + " elements; use nzb_norm with a caller-provided buffer");
+  double* scratch = nullptr;
+  if (scratch_address(&scratch)) return -1;
+  const int64_t nb = blocks_for(E);
+  // every slot the finalize reads is written first, so nothing is cleared
+  k_norm_partial<<<(unsigned)nb, NT, 0, (cudaStream_t)stream>>>(A, E, np, w4[0], w4[1], w4[2], w4[3], scratch);
+  if (launch_check("norm_noalloc launch")) return -1;
+  return nzb_norm_finalize(scratch, nb, 4.0 * (double)E * np, out, stream);
 }
 
 int nzb_solver_create(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_buffers* buf, int scheme_ssprk3,

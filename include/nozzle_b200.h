@@ -167,6 +167,23 @@ int nzb_norm_finalize(const double* partial, int64_t n_partial, double count, do
 int nzb_norm(const double* A, int64_t n_elem, int np, const double* w4, double* partial, double* out,
              void* stream);
 
+/* nzb_norm without a scratch argument, for callers that cannot allocate
+ * device memory: a host application that passes this library only buffers
+ * from a fixed pool it manages itself, or a loop that must never enter the
+ * CUDA allocator (cudaFree, for one, synchronizes the whole device).  It has
+ * no counterpart in the reference solver.
+ *
+ * The per-block partial sums go to a fixed array in the library's device
+ * memory (512 KiB on every GPU that loads the library, held until exit), so
+ * n_elem is limited to 8,388,608; a larger n_elem is rejected with an error
+ * and nothing is launched.  No call allocates or frees memory.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All
+ * calls share the array, which keeps the last call's partial sums -- each call
+ * overwrites every slot it reads -- and calls that overlap on the GPU (other
+ * streams, other host threads) race on it. */
+int nzb_norm_noalloc(const double* A, int64_t n_elem, int np, const double* w4, double* out, void* stream);
+
 /* A steady-march solver over caller-owned buffers.  Every step maps S0 -> S0
  * (scratch S1, S2); a chunk of n steps is captured once as a CUDA graph and
  * replayed.  res (device double) receives the norm of the last step's stage-1
