@@ -156,11 +156,11 @@ def solve_device(bk, U0_dev_soa, opts, scale, torch):
     return converged, done, res, launches
 
 
-def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind):
-    ops, U = microbench_case()
+def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
+    ops, U = microbench_case(nx, nr)
     E = ops.n_elem
-    out = {"workload": f"residual microbench: {E} straight-sided cubic triangles (Np=10), unit rectangle 1000x500 cells",
-           "l2": "state 320 MB > 126 MB L2", "kernels": {}}
+    out = {"workload": f"residual microbench: {E} straight-sided cubic triangles (Np=10), unit rectangle {nx}x{nr} cells",
+           "l2": f"state {U.nbytes / 1e6:.0f} MB vs 126 MB L2", "kernels": {}}
     results = {}
     for flux in ("roe", "hllc", "ausmup"):
         bk = B(ops, cfg.FlowConditions(flux=flux), cfg.SolverOptions(cfl=0.5))
@@ -377,7 +377,9 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-micro", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--micro-only", action="store_true", help="run only the 1M-element microbench (profiling)")
+    ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
+    ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
+    ap.add_argument("--micro-nr", type=int, default=500, help="microbench cells across")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -399,7 +401,8 @@ def main():
     pkg("build").build()
     if args.micro_only:
         peak, kind = load_peaks()
-        print(json.dumps(microbench(torch, pkg("capi"), pkg("backend").B200Backend, pkg("config"), peak, kind)))
+        print(json.dumps(microbench(torch, pkg("capi"), pkg("backend").B200Backend, pkg("config"), peak, kind,
+                                    args.micro_nx, args.micro_nr)))
         return
     line = run_ours(args, rank, world, torch, dist)
     if rank == 0:

@@ -266,6 +266,52 @@ def batch_cases():
     print("wrote batch_cases.json")
 
 
+def _sweep_point(args):
+    """One design point through the reference's own solve (one Numba thread per worker)."""
+    k, el, p, r, ar, pb, max_it = args
+    import numba
+
+    numba.set_num_threads(1)
+    from src.api import solve_nozzle
+    from src.post.postprocess import performance
+
+    try:
+        res = solve_nozzle(element=el, order=p, refine=r, area_ratio=ar, back_pressure_ratio=pb, flux="hllc",
+                           tolerance=1e-10, max_iterations=max_it, limiter="positivity", backend="numba", verbose=False)
+    except ValueError as exc:
+        return {"point": k, "refused": True, "message": str(exc)[:80]}
+    row = {"point": k, "refused": False, "converged": bool(res.converged), "iterations": int(res.iterations),
+           "residual": float(res.residual), "message": res.message[:120]}
+    if res.converged:
+        perf = performance(res)
+        row.update(thrust=perf.thrust, mass_flow_in=perf.mass_flow_in, exit_mach=perf.exit_mach_area_averaged)
+    return row
+
+
+def sweep_outcomes(n=256, seed=0, max_it=20000, workers=6):
+    """The reference's outcome for every point of the sampled design sweep.
+
+    The points come from the same sampler as the batched sweep (area ratio
+    U[1.5, 4], back pressure U[0.1, 0.9], p in {1, 2, 3}, refine in {1, 2, 3},
+    tri/quad 50/50, seed 0), each solved by the reference's solve_nozzle with
+    HLLC, the positivity limiter, tolerance 1e-10 and an iteration cap.
+    """
+    import importlib
+    import json
+    from concurrent.futures import ProcessPoolExecutor
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    pts = importlib.import_module("2d_nozzle_b200.sweep").sample_points(n, seed)
+    jobs = [(k, pt.element, pt.order, pt.refine, pt.area_ratio, pt.back_pressure_ratio, max_it) for k, pt in enumerate(pts)]
+    # the heaviest first, so the pool drains evenly
+    jobs.sort(key=lambda j: -(4 ** j[3]) * (j[2] + 1) ** 2)
+    with ProcessPoolExecutor(workers) as ex:
+        rows = sorted(ex.map(_sweep_point, jobs), key=lambda r: r["point"])
+    with open(os.path.join(HERE, "sweep_reference.json"), "w") as f:
+        json.dump({"n": n, "seed": seed, "max_iterations": max_it, "rows": rows}, f, indent=0)
+    print("wrote sweep_reference.json")
+
+
 if __name__ == "__main__":
     import src  # noqa: F401  -- fails loudly when the reference is not on PYTHONPATH
 
@@ -280,3 +326,5 @@ if __name__ == "__main__":
         config3()
     if "batch" in which:
         batch_cases()
+    if "sweep" in which:
+        sweep_outcomes()
