@@ -88,6 +88,8 @@ class BatchSolver:
         p_back = np.zeros(n)
         self.meshes, self.buffers, self.phys, self.offsets, self.factors = [], [], [], [], []
         self._keep = []
+        self.U0_soa = []  # each bucket's initial state, kept for reset()
+        self.h2d_bytes = 0  # host -> device bytes of the set-up (states, geometry, connectivity)
         g_off = 0
         for key, mem in zip(self.bucket_keys, self.members):
             parts = [host_arrays(instances[i].ops) for i in mem]
@@ -121,6 +123,8 @@ class BatchSolver:
             dt = torch.zeros(dm.E, dtype=torch.float64, device=dev)
             U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])
             dm.pack(U0, S[0])
+            self.U0_soa.append(S[0].clone())
+            self.h2d_bytes += U0.nbytes + sum(a.nbytes for a in arrays.values() if isinstance(a, np.ndarray))
             bf = capi.Buffers()
             bf.S0, bf.S1, bf.S2 = (x.data_ptr() for x in S)
             bf.dt = dt.data_ptr()
@@ -178,6 +182,7 @@ class BatchSolver:
         self.handle = h.value
         self.done = 0
         self.chunks = 0
+        self.launches = 0
 
     def __del__(self):
         if getattr(self, "handle", None):
@@ -187,11 +192,27 @@ class BatchSolver:
     def _stream(self):
         return self.torch.cuda.current_stream(self.device).cuda_stream
 
+    def launches_per_chunk(self, n: int) -> int:
+        """Kernel launches of one n-step chunk: 3 stages (SSP-RK3) or a stage and a copy (Euler) per
+        bucket and step, plus the check."""
+        return sum((3 if dm.order > 0 else 2) * n for dm in self.meshes) + 1
+
     def step_chunk(self, n: int, first: bool) -> int:
         capi.check(self.lib.nzb_batch_run(self.handle, int(n), 1 if first else 0, self._stream), "nzb_batch_run")
         self.done += n
         self.chunks += 1
+        self.launches += self.launches_per_chunk(n)
         return int(self.t["n_running"].item())
+
+    def reset(self) -> None:
+        """Put every instance back at its initial state with a fresh march record."""
+        for (bf, S), U0 in zip(self.buffers, self.U0_soa):
+            S[0].copy_(U0)
+        for k in ("status", "iterations", "res0", "res", "window", "window_count", "elem_norm", "n_running"):
+            self.t[k].zero_()
+        self.done = 0
+        self.chunks = 0
+        self.launches = 0
 
     def run(self) -> int:
         """March every instance to retirement; returns the number of chunks."""

@@ -1,14 +1,22 @@
-"""Benchmark: steady solves/s on one B200, plus the residual-kernel HBM roofline.
+"""Benchmark: batched steady design-sweep solves/s on one B200, with the plain
+(one solve at a time) rate on the same points, the residual-kernel roofline and
+the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one steady solve of the reference nozzle case (smooth contour,
-area ratio 2.5, p = 1 triangles, refine 1 = 560 elements, Roe, cfl 0.5,
-positivity limiter, SSP-RK3, from its quasi-1D initial state to a scaled
-residual of 1e-10: 11,751 iterations).  ``value`` times it with the state
-resident in HBM (one 8-byte residual read back per 50-step convergence check);
-``e2e`` times it through the public backend API the reference's march calls,
-``run(U_host, n)``, which copies the state in and out every chunk.
+A step is one batched sweep: 256 operating points sampled with seed 0 (area
+ratio U[1.5, 4], back-pressure ratio U[0.1, 0.9], p in {1, 2, 3}, refine in
+{1, 2, 3}, triangles / quadrilaterals 50/50, bell contour, HLLC, positivity
+limiter, SSP-RK3, tolerance 1e-10).  Points that stand a normal shock in the
+nozzle are refused on the host, as the reference's sweep records them; every
+other point is marched from its quasi-1D initial state, all together, each to
+its own retirement (converged, stalled, diverged, non-finite or the iteration
+cap).  ``value`` counts converged solves per second with every state resident
+in HBM; ``e2e`` times the public path -- BatchSolver set-up from host arrays
+(states, geometry, connectivity copied in), the march, and every state and
+status copied back.  ``plain`` marches a subset one instance at a time through
+the single-solve backend and the same subset as a batch: their ratio is the
+batched speed-up over the same attempted set.
 
 ``roofline`` is measured on the residual-kernel microbenchmark: 1,000,000
 straight-sided cubic triangles (Np = 10) on the unit rectangle, states drawn
@@ -16,8 +24,9 @@ per node (density lognormal(0, 0.3), Mach U[0.2, 3] in a random direction,
 pressure lognormal(0, 0.5)), one residual per flux and one SSP-RK3 step with
 the positivity limiter; the state (320 MB) is larger than L2.
 
-Multi-GPU: design points are independent, so N GPUs run N replicas
-(weak scaling); ``value`` = all ranks' solves / the slowest rank's time.
+Multi-GPU: design points are independent, so N GPUs run N replicas of the
+sweep (weak scaling); ``value`` = all ranks' converged solves / the slowest
+rank's time.
 """
 
 from __future__ import annotations
@@ -42,16 +51,6 @@ def pkg(name=""):
 
 
 # ------------------------------------------------------------------ workloads
-def config1_case():
-    g = np.load(os.path.join(GOLDEN, "config1.npz"))
-    cfg = pkg("config")
-    topo, _, _ = pkg("mesh").channel_topology("tri", refine=1)
-    ops = pkg("operators").build_operators(topo, g["node_coords"], 1)
-    flow = cfg.FlowConditions(flux="roe", back_pressure_ratio=0.15)
-    opts = cfg.SolverOptions(cfl=0.5, tolerance=1e-10, limiter="positivity", scheme="ssprk3", print_interval=0)
-    return ops, flow, opts, g
-
-
 def microbench_state(n_elem, nbf, gamma=1.4, seed=0):
     rng = np.random.default_rng(seed)
     shape = (n_elem, nbf)
@@ -227,44 +226,70 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
     return out
 
 
-def cpu_baseline_oracle(seconds=15.0):
-    """The oracle (NumPy restatement) marching config 1 for a bounded number of iterations."""
+SWEEP_POINTS = 256
+SWEEP_SEED = 0
+
+
+def sweep_workload(max_iterations, n_points=SWEEP_POINTS):
+    sweep = pkg("sweep")
+    points = sweep.sample_points(n_points, SWEEP_SEED)
+    insts, index, refused = sweep.build_instances(points, max_iterations=max_iterations)
+    return points, insts, index, refused
+
+
+def oracle_costs(insts, seconds):
+    """Seconds per SSP-RK3 iteration of the NumPy oracle for each (kind, order, n_elem) class of the sweep,
+    timed on a few iterations of one member of each class within a total budget of about ``seconds``."""
     from oracle import dg_oracle as orc
 
-    ops, flow, opts, g = config1_case()
-    st = orc.Stepper(ops, flow, opts)
-    U = g["U0"].copy()
-    st.run(U, 2)
-    t0 = time.perf_counter()
-    n = 0
-    while time.perf_counter() - t0 < seconds:
-        U, _ = st.run(U, 5)
-        n += 5
-    dt = (time.perf_counter() - t0) / n
-    iters = int(g["iterations"])
-    return {"value": 1.0 / (dt * iters), "unit": "solves/s", "cores": 1, "kind": "port",
-            "sample": f"{n} SSP-RK3 iterations of the config-1 march ({dt * 1e3:.2f} ms each), scaled to the "
-                      f"reference's {iters} iterations per solve; NumPy oracle, single thread"}
+    classes = {}
+    for i, inst in enumerate(insts):
+        classes.setdefault((inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem), i)
+    per = seconds / max(1, len(classes))
+    cost = {}
+    for key, i in classes.items():
+        inst = insts[i]
+        st = orc.Stepper(inst.ops, inst.flow, inst.opts)
+        U = np.asarray(inst.U0, float).copy()
+        U, _ = st.run(U, 1)
+        t0 = time.perf_counter()
+        n = 0
+        while n < 2 or time.perf_counter() - t0 < per:
+            U, _ = st.run(U, 1)
+            n += 1
+        cost[key] = (time.perf_counter() - t0) / n
+    return cost, len(classes)
+
+
+def cpu_time_for(insts, iterations, cost):
+    return float(sum(it * cost[(inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem)]
+                     for inst, it in zip(insts, iterations)))
+
+
+def plain_solve(inst, torch):
+    """One instance through the single-solve backend, state resident in HBM."""
+    cfg = pkg("config")
+    bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts)
+    U0 = bk.mesh.pack(inst.U0).clone()
+    scale = cfg.residual_scale(inst.flow, inst.length)
+    return bk, U0, scale
 
 
 def run_ours(args, rank, world, torch, dist):
     capi = pkg("capi")
-    cfg = pkg("config")
-    B = pkg("backend").B200Backend
-    march = pkg("march")
+    BatchSolver = pkg("batch").BatchSolver
     peak, peak_kind = load_peaks()
-    ops, flow, opts, g = config1_case()
-    bk = B(ops, flow, opts)
-    scale = cfg.residual_scale(flow, float(g["length"]))
-    U0 = bk.mesh.pack(g["U0"]).clone()
+    points, insts, index, refused = sweep_workload(args.max_iterations, args.points)
+    solver = BatchSolver(insts)
     flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
 
-    for _ in range(max(3, args.warmup)):
-        conv, its, res, _ = solve_device(bk, U0, opts, scale, torch)
-    if not conv or its != int(g["iterations"]):
-        raise RuntimeError(f"warm-up solve did not reproduce the reference: converged={conv}, iterations={its}")
+    W = max(3, args.warmup)
+    for _ in range(W):
+        solver.reset()
+        solver.run()
+    ref_out = [(r.status, r.iterations) for r in solver.results(with_state=False)]
 
     times, launches = [], 0
     if dist is not None:
@@ -272,99 +297,158 @@ def run_ours(args, rank, world, torch, dist):
     torch.cuda.synchronize()
     with Clocks(torch.cuda.current_device()) as clk:
         for _ in range(args.steps):
+            solver.reset()
             flush_l2(torch, flush)
+            torch.cuda.synchronize()
             ev[0].record(st)
-            conv, its, res, nl = solve_device(bk, U0, opts, scale, torch)
+            solver.run()
             ev[1].record(st)
             torch.cuda.synchronize()
             times.append(ev[0].elapsed_time(ev[1]) * 1e-3)
-            launches += nl
-            assert conv and its == int(g["iterations"])
+            launches += solver.launches
+    res = solver.results(with_state=False)
+    if [(r.status, r.iterations) for r in res] != ref_out:
+        raise RuntimeError("the batched sweep is not deterministic across repeats")
     if dist is not None:
         dist.barrier()
+    n_conv = sum(r.converged for r in res)
     t_rank = float(np.sum(times))
     t_max = t_rank
     if dist is not None:
         tt = torch.tensor([t_rank], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_max = float(tt.item())
-    value = world * args.steps / t_max
+    value = world * n_conv * args.steps / t_max
+    outcomes = {}
+    for r in res:
+        outcomes[r.status] = outcomes.get(r.status, 0) + 1
+    outcomes["refused"] = len(refused)
 
-    # end to end through the public API: host state in and out every chunk
-    pin = torch.from_numpy(g["U0"].copy()).pin_memory()
-    e2e_times = []
-    state_bytes = g["U0"].nbytes
-    chunks = None
-    for k in range(args.steps + 1):
-        bk2 = bk
-        bk2.n_limited = bk2.n_limit_calls = bk2.n_mean_repaired = 0
+    # end to end: set-up from host arrays, march, every state and status back
+    e2e_t, h2d, d2h = [], 0, 0
+    for k in range(2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        U0h = pin.numpy()
-        r = march.solve(bk2, U0h, length=float(g["length"]))
+        sv = BatchSolver(insts)
+        sv.run()
+        out = sv.results(with_state=True)
         torch.cuda.synchronize()
+        t1 = time.perf_counter()
         if k > 0:
-            e2e_times.append(time.perf_counter() - t0)
-        chunks = len(r.history_iterations)
-        assert r.converged and r.iterations == int(g["iterations"])
-    e2e_value = world / float(np.mean(e2e_times))
+            e2e_t.append(t1 - t0)
+        h2d = sv.h2d_bytes
+        d2h = sum(o.U.nbytes for o in out) + 4 * 2 * len(out) + 8 * 2 * len(out) + 4 * sv.chunks
+        del sv
+    e2e_value = world * n_conv / float(np.mean(e2e_t))
+
+    # plain (one solve at a time) vs batched on the same subset
+    sub = insts[:: args.plain_stride]
+    p_times, p_conv, p_its = [], 0, []
+    for inst in sub:
+        bk, U0, scale = plain_solve(inst, torch)
+        bk._S[0].copy_(U0)
+        bk.run_device(1)  # warm: capture the 1-step and check-interval graphs
+        bk.run_device(inst.opts.check_interval)
+        torch.cuda.synchronize()
+        ev[0].record(st)
+        conv, its, _, _ = solve_device(bk, U0, inst.opts, scale, torch)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        p_times.append(ev[0].elapsed_time(ev[1]) * 1e-3)
+        p_conv += conv
+        p_its.append(its)
+        del bk
+    sb = BatchSolver(sub)
+    sb.run()
+    sb.reset()
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    sb.run()
+    ev[1].record(st)
+    torch.cuda.synchronize()
+    b_time = ev[0].elapsed_time(ev[1]) * 1e-3
+    b_res = sb.results(with_state=False)
+    b_conv = sum(r.converged for r in b_res)
+    if [r.iterations for r in b_res] != p_its:
+        raise RuntimeError("plain and batched solves took different iteration counts")
+    plain = {"instances": len(sub), "converged": int(p_conv), "plain_seconds": float(np.sum(p_times)),
+             "batched_seconds": b_time, "plain_solves_per_s": p_conv / float(np.sum(p_times)),
+             "batched_solves_per_s": b_conv / b_time, "speedup": float(np.sum(p_times)) / b_time,
+             "subset": f"every {args.plain_stride}th built point"}
 
     line = {
-        "metric": "steady solves/s at 1e-10 residual (plain, one solve at a time; batched sweep not yet built)",
+        "metric": "batched steady design-sweep solves/s at 1e-10 scaled residual (converged solves)",
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
         "steps": args.steps,
-        "warmup": max(3, args.warmup),
+        "warmup": W,
         "ms_per_step": 1e3 * t_max / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic: the reference's own mesh and quasi-1D initial state for config 1 (fixtures in tests/golden)",
-        "config": {"workload": "config1: smooth AR 2.5, tri p=1, refine 1 (560 elements), Roe, cfl 0.5, tol 1e-10",
-                   "iterations_per_solve": int(g["iterations"]), "l2": "flushed (256 MB write) between solves",
+        "data": "synthetic: sampled operating points (seed 0) on the reference's own mesh generator and quasi-1D "
+                "initial states, built on the host",
+        "config": {"workload": f"design sweep: {len(points)} points, {len(insts)} built, {len(refused)} refused "
+                               f"(shock in nozzle); tri/quad p 1-3 refine 1-3, bell contour, HLLC, positivity "
+                               f"limiter, tol 1e-10, cap {args.max_iterations} iterations",
+                   "elements": int(solver.n_elem), "buckets": len(solver.meshes), "outcomes": outcomes,
+                   "converged_per_step": int(n_conv), "l2": "flushed (256 MB write) before each sweep",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(state_bytes * chunks),
-                "d2h_bytes_per_step": int((state_bytes + 8) * chunks), "path": "march -> B200Backend.run(host U, 50)"},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "path": "BatchSolver(host instances) -> run() -> results(with_state=True)"},
+        "plain": plain,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
     if rank == 0 and not args.no_micro:
-        mb = microbench(torch, capi, B, cfg, peak, peak_kind)
+        mb = microbench(torch, capi, pkg("backend").B200Backend, pkg("config"), peak, peak_kind)
         line["roofline"] = mb.pop("roofline")
         line["microbench"] = mb
     if rank == 0:
-        line["cpu_baseline"] = cpu_baseline_oracle(args.cpu_seconds)
+        cost, ncls = oracle_costs(insts, args.cpu_seconds)
+        t_cpu = cpu_time_for(insts, [r.iterations for r in res], cost)
+        line["cpu_baseline"] = {
+            "value": n_conv / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": f"NumPy oracle SSP-RK3 iterations timed on one member of each of the sweep's {ncls} "
+                      f"(kind, order, mesh) classes (~{args.cpu_seconds:.0f} s in all), scaled by every instance's "
+                      f"iteration count on the GPU; single thread"}
+    del solver
     return line
 
 
 def run_reference(args):
-    """The reference's CPU path (the NumPy oracle restating it) on config 1."""
-    from oracle import dg_oracle as orc
-
-    ops, flow, opts, g = config1_case()
-    st = orc.Stepper(ops, flow, opts)
-    U = g["U0"].copy()
-    sample = 25
-    for _ in range(args.warmup):
-        U, _ = st.run(U, sample)
+    """The reference's CPU path on the same sweep: the NumPy oracle's per-iteration cost for each mesh class,
+    times the iteration count the reference solver itself took on each point (tests/golden/sweep_reference.json)."""
+    path = os.path.join(GOLDEN, "sweep_reference.json")
+    base = {"impl": "reference", "metric": "batched steady design-sweep solves/s at 1e-10 scaled residual (converged solves)"}
+    if not os.path.exists(path):
+        return {**base, "unavailable": "tests/golden/sweep_reference.json (the reference's sweep outcomes) is missing"}
+    with open(path) as f:
+        ref = json.load(f)
+    points, insts, index, refused = sweep_workload(ref["max_iterations"], ref["n"])
+    rows = {r["point"]: r for r in ref["rows"]}
+    its = [rows[k]["iterations"] for k in index]
+    n_conv = sum(1 for k in index if rows[k].get("converged"))
     ts = []
+    for _ in range(args.warmup):
+        oracle_costs(insts, 2.0)
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        U, _ = st.run(U, sample)
+        cost, ncls = oracle_costs(insts, args.cpu_seconds / max(1, args.steps))
         ts.append(time.perf_counter() - t0)
-    per_it = float(np.sum(ts)) / (sample * args.steps)
-    iters = int(g["iterations"])
-    value = 1.0 / (per_it * iters)
+    t_cpu = cpu_time_for(insts, its, cost)
+    value = n_conv / t_cpu
+    sample = (f"each step times NumPy-oracle SSP-RK3 iterations on one member of each of {ncls} mesh classes; the "
+              f"sweep's CPU time is that cost times the reference solver's own iteration count on each point")
     return {
-        "impl": "reference", "metric": "steady solves/s at 1e-10 residual (plain, one solve at a time; batched sweep not yet built)",
-        "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        **base, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(ts)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "the reference's config-1 mesh and initial state",
-        "config": {"workload": "config1: smooth AR 2.5, tri p=1, refine 1 (560 elements), Roe, cfl 0.5, tol 1e-10"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
-                         "sample": f"each step = {sample} SSP-RK3 iterations of the NumPy oracle, scaled to {iters} per solve"},
+        "dtype": "f64", "data": "the same sampled sweep (seed 0), reference outcomes from its own solver",
+        "config": {"workload": f"design sweep: {len(points)} points, {len(insts)} built, {len(refused)} refused; "
+                               f"reference converged {n_conv}"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -372,11 +456,14 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--points", type=int, default=SWEEP_POINTS, help="operating points sampled for the sweep")
+    ap.add_argument("--max-iterations", type=int, default=20000, help="iteration cap of every instance")
+    ap.add_argument("--plain-stride", type=int, default=8, help="plain-vs-batched subset: every n-th built point")
     ap.add_argument("--no-micro", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=18.0)
     ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
     ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
     ap.add_argument("--micro-nr", type=int, default=500, help="microbench cells across")
