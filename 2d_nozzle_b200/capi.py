@@ -117,6 +117,58 @@ class BatchMarch(C.Structure):
     ]
 
 
+class AdjointArgs(C.Structure):
+    _fields_ = [
+        ("mode", I32),
+        ("stage", I32),
+        ("U", P),
+        ("lam", P),
+        ("seed", P),
+        ("out", P),
+        ("lam0", P),
+        ("dt", P),
+        ("f0", P),
+        ("f1", P),
+        ("f2", P),
+        ("norm_partial", P),
+        ("elem_norm", P),
+    ]
+
+
+class AdjointBuffers(C.Structure):
+    _fields_ = [
+        ("U", P),
+        ("seed", P),
+        ("lam", P),
+        ("Y1", P),
+        ("Y2", P),
+        ("f0", P),
+        ("f1", P),
+        ("f2", P),
+        ("dt", P),
+    ]
+
+
+class AdjointMarch(C.Structure):
+    _fields_ = [
+        ("n_inst", I64),
+        ("inst_begin", P),
+        ("inst_end", P),
+        ("inst_count", P),
+        ("elem_norm", P),
+        ("status", P),
+        ("iterations", P),
+        ("res0", P),
+        ("res", P),
+        ("n_running", P),
+        ("tolerance", C.c_double),
+        ("max_iterations", I32),
+        ("reserved", I32),
+    ]
+
+
+ADJ_VJP, ADJ_DEFECT, ADJ_RATE, ADJ_RK4 = 0, 1, 2, 3
+
 # (name, restype, argtypes) of every exported symbol
 SIGNATURES = [
     ("nzb_version", C.c_int, []),
@@ -141,6 +193,13 @@ SIGNATURES = [
                                    C.POINTER(BatchMarch), C.POINTER(P)]),
     ("nzb_batch_run", C.c_int, [P, C.c_int, C.c_int, P]),
     ("nzb_batch_destroy", C.c_int, [P]),
+    ("nzb_vjp", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(AdjointArgs), P]),
+    ("nzb_vjp_coords", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P, P, P, P]),
+    ("nzb_local_dt", C.c_int, [C.POINTER(Mesh), P, C.c_double, P, P]),
+    ("nzb_adjoint_create", C.c_int, [C.c_int, C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(AdjointBuffers), P,
+                                     C.POINTER(AdjointMarch), C.POINTER(P)]),
+    ("nzb_adjoint_run", C.c_int, [P, C.c_int, P]),
+    ("nzb_adjoint_destroy", C.c_int, [P]),
 ]
 
 _lib = None

@@ -14,6 +14,7 @@
 #include <utility>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "element.cuh"
 #include "nozzle_b200.h"
 
@@ -432,6 +433,203 @@ static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
   return 0;
 }
 
+// ---- adjoint ------------------------------------------------------------------
+template <int K, int P, bool AFF>
+static int launch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
+  const int64_t nb = element_blocks(m);
+  if (nb > 0x7fffffff) return fail("too many elements for one launch");
+  k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  return launch_check("vjp kernel launch");
+}
+
+static int dispatch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
+#define NZB_CASE(K, P)                                                       \
+  if (m.kind == K && m.order == P) {                                         \
+    if (K == 0 && m.affine) return launch_vjp<K, P, (K == 0)>(m, ph, w, st); \
+    return launch_vjp<K, P, false>(m, ph, w, st);                            \
+  }
+  NZB_CASE(0, 0)
+  NZB_CASE(0, 1)
+  NZB_CASE(0, 2)
+  NZB_CASE(0, 3)
+  NZB_CASE(1, 0)
+  NZB_CASE(1, 1)
+  NZB_CASE(1, 2)
+  NZB_CASE(1, 3)
+#undef NZB_CASE
+  return fail("unsupported kind/order");
+}
+
+static int dispatch_vjp_coords(const nzb_mesh& m, const nzb_physics& ph, const CoordWork& w, cudaStream_t st) {
+  const int64_t nb = (m.n_elem + 127) / 128;
+  if (nb > 0x7fffffff) return fail("too many elements for one launch");
+#define NZB_CASE(K, P)                                          \
+  if (m.kind == K && m.order == P) {                            \
+    k_vjp_coords<K, P><<<(unsigned)nb, 128, 0, st>>>(m, ph, w); \
+    return launch_check("vjp_coords kernel launch");            \
+  }
+  NZB_CASE(0, 0)
+  NZB_CASE(0, 1)
+  NZB_CASE(0, 2)
+  NZB_CASE(0, 3)
+  NZB_CASE(1, 0)
+  NZB_CASE(1, 1)
+  NZB_CASE(1, 2)
+  NZB_CASE(1, 3)
+#undef NZB_CASE
+  return fail("unsupported kind/order");
+}
+
+__global__ void k_local_dt(const double* __restrict__ area, const double* __restrict__ wave, int64_t E, double coef,
+                           double* __restrict__ dt) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const double d = wave[e] < FLOOR ? FLOOR : wave[e];
+  dt[e] = coef * 2.0 * area[e] / d;
+}
+
+// One block per instance: rms of the defect in a fixed order, then the adjoint
+// march's tests (src/sensitivity.py:366-383).  n_steps = 0 records res0.
+__global__ void __launch_bounds__(256) k_adjoint_check(nzb_adjoint_march am, int n_steps) {
+  const int64_t inst = blockIdx.x;
+  if (inst >= am.n_inst || am.status[inst] != 0) return;
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int64_t e = am.inst_begin[inst] + threadIdx.x; e < am.inst_end[inst]; e += 256) acc += am.elem_norm[e];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double res = sqrt(red[0] / am.inst_count[inst]);
+  int st = 0;
+  if (n_steps == 0) {
+    am.res0[inst] = res;
+    am.res[inst] = res;
+    am.iterations[inst] = 0;
+    if (!isfinite(res))
+      st = 2;
+    else if (res == 0.0)
+      st = 1;
+  } else {
+    const int done = am.iterations[inst] + n_steps;
+    am.iterations[inst] = done;
+    am.res[inst] = res;
+    if (!isfinite(res))
+      st = 2;
+    else if (res <= am.tolerance * am.res0[inst])
+      st = 1;
+    else if (done >= am.max_iterations)
+      st = 5;
+  }
+  am.status[inst] = st;
+  if (st == 0) atomicAdd(am.n_running, 1);
+}
+
+struct AdjBatch {
+  std::vector<nzb_mesh> mesh;
+  std::vector<nzb_physics> phys;
+  std::vector<nzb_adjoint_buffers> buf;
+  std::vector<int64_t> offset;
+  nzb_adjoint_march am;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<cudaStream_t> bstream;
+  std::vector<cudaEvent_t> bdone;
+  cudaEvent_t fork = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;  // key: steps per chunk
+};
+
+static int enqueue_adjoint_step(const AdjBatch& A, size_t b, cudaStream_t st) {
+  const nzb_adjoint_buffers& bf = A.buf[b];
+  AdjWork w{};
+  w.mode = ADJ_RK4;
+  w.U = bf.U;
+  w.seed = bf.seed;
+  w.lam0 = bf.lam;
+  w.dt = bf.dt;
+  w.f0 = bf.f0;
+  w.f1 = bf.f1;
+  w.f2 = bf.f2;
+  // stage inputs alternate between two buffers, so no stage reads what it writes
+  const double* in[4] = {bf.lam, bf.Y1, bf.Y2, bf.Y1};
+  double* outp[4] = {bf.Y1, bf.Y2, bf.Y1, nullptr};
+  for (int k = 0; k < 4; ++k) {
+    w.stage = k;
+    w.lam = in[k];
+    w.out = outp[k];
+    if (dispatch_vjp(A.mesh[b], A.phys[b], w, st)) return -1;
+  }
+  return 0;
+}
+
+static int enqueue_adjoint_defect(const AdjBatch& A, size_t b, cudaStream_t st) {
+  const nzb_adjoint_buffers& bf = A.buf[b];
+  AdjWork w{};
+  w.mode = ADJ_DEFECT;
+  w.U = bf.U;
+  w.seed = bf.seed;
+  w.lam = bf.lam;
+  w.elem_norm = A.am.elem_norm + A.offset[b];
+  return dispatch_vjp(A.mesh[b], A.phys[b], w, st);
+}
+
+static int adjoint_graph(AdjBatch& A, int n, cudaGraphExec_t* out) {
+  auto it = A.graphs.find(n);
+  if (it != A.graphs.end()) {
+    *out = it->second;
+    return 0;
+  }
+  cudaGraph_t g = nullptr;
+  if (cuda_check(cudaStreamBeginCapture(A.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return -1;
+  int rc = cuda_check(cudaEventRecord(A.fork, A.stream), "fork record");
+  for (size_t b = 0; b < A.mesh.size() && rc == 0; ++b) {
+    rc = cuda_check(cudaStreamWaitEvent(A.bstream[b], A.fork, 0), "fork wait");
+    for (int i = 0; i < n && rc == 0; ++i) rc = enqueue_adjoint_step(A, b, A.bstream[b]);
+    if (rc == 0) rc = enqueue_adjoint_defect(A, b, A.bstream[b]);
+    if (rc == 0) rc = cuda_check(cudaEventRecord(A.bdone[b], A.bstream[b]), "join record");
+    if (rc == 0) rc = cuda_check(cudaStreamWaitEvent(A.stream, A.bdone[b], 0), "join wait");
+  }
+  if (rc == 0) rc = cuda_check(cudaMemsetAsync(A.am.n_running, 0, sizeof(int32_t), A.stream), "memset");
+  if (rc == 0) {
+    k_adjoint_check<<<(unsigned)A.am.n_inst, 256, 0, A.stream>>>(A.am, n);
+    rc = launch_check("adjoint check");
+  }
+  const cudaError_t end = cudaStreamEndCapture(A.stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return -1;
+  }
+  if (cuda_check(end, "end capture")) return -1;
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t inst = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (cuda_check(inst, "graph instantiate")) return -1;
+  A.graphs[n] = ex;
+  *out = ex;
+  return 0;
+}
+
+static AdjWork adj_work(const nzb_adjoint_args& a) {
+  AdjWork w{};
+  w.mode = a.mode;
+  w.stage = a.stage;
+  w.U = a.U;
+  w.lam = a.lam;
+  w.seed = a.seed;
+  w.out = a.out;
+  w.lam0 = a.lam0;
+  w.dt = a.dt;
+  w.f0 = a.f0;
+  w.f1 = a.f1;
+  w.f2 = a.f2;
+  w.norm_partial = a.norm_partial;
+  w.elem_norm = a.elem_norm;
+  return w;
+}
+
 // ---- the norm without caller-provided scratch ------------------------------------
 // Partial sums of nzb_norm_noalloc live in this file-scope array: one slot per
 // block of the partial-sum kernel, 128 elements per block.  Every GPU that
@@ -744,6 +942,145 @@ int nzb_batch_destroy(nzb_batch* batch) {
   for (auto s : B->bstream) cudaStreamDestroy(s);
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
+  return 0;
+}
+
+int nzb_vjp(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_adjoint_args* a, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !a || !a->U || !a->lam) return fail("vjp: null argument");
+  switch (a->mode) {
+    case NZB_ADJ_VJP:
+    case NZB_ADJ_RATE:
+      if (!a->out) return fail("vjp: out is null");
+      if (a->mode == NZB_ADJ_RATE && !a->seed) return fail("vjp: rate needs seed");
+      if (a->out == a->lam || a->out == a->U) return fail("vjp: out must not alias lam or U");
+      break;
+    case NZB_ADJ_DEFECT:
+      if (!a->seed) return fail("vjp: defect needs seed");
+      if (a->out && (a->out == a->lam || a->out == a->U)) return fail("vjp: out must not alias lam or U");
+      break;
+    case NZB_ADJ_RK4:
+      if (!a->seed || !a->lam0 || !a->dt || !a->f0 || !a->f1 || !a->f2)
+        return fail("vjp: rk4 needs seed, lam0, dt, f0..f2");
+      if (a->stage < 0 || a->stage > 3) return fail("vjp: rk4 stage must be 0..3");
+      if (a->stage < 3 && (!a->out || a->out == a->lam || a->out == a->lam0))
+        return fail("vjp: rk4 out missing or aliased");
+      if (a->stage == 3 && a->lam == a->lam0) return fail("vjp: rk4 stage 3 input must not alias lam0");
+      break;
+    default:
+      return fail("vjp: unknown mode");
+  }
+  return dispatch_vjp(*mesh, *phys, adj_work(*a), (cudaStream_t)stream);
+}
+
+int nzb_vjp_coords(const nzb_mesh* mesh, const nzb_physics* phys, const double* U, const double* lam,
+                   const double* verts, const double* dgs, double* gvert, double* gpb, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !U || !lam || !verts || !dgs || !gvert) return fail("vjp_coords: null argument");
+  CoordWork w{};
+  w.U = U;
+  w.lam = lam;
+  w.verts = verts;
+  w.gvert = gvert;
+  w.gpb = gpb;
+  for (int f = 0; f < 4; ++f)
+    for (int v = 0; v < 4; ++v) w.dgs[f][v] = dgs[4 * f + v];
+  return dispatch_vjp_coords(*mesh, *phys, w, (cudaStream_t)stream);
+}
+
+int nzb_local_dt(const nzb_mesh* mesh, const double* wave, double coefficient, double* dt, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!wave || !dt) return fail("local_dt: null argument");
+  const int64_t E = mesh->n_elem;
+  k_local_dt<<<(unsigned)((E + 127) / 128), 128, 0, (cudaStream_t)stream>>>(mesh->area, wave, E, coefficient, dt);
+  return launch_check("local dt launch");
+}
+
+int nzb_adjoint_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics* phys,
+                       const nzb_adjoint_buffers* buffers, const int64_t* elem_offset,
+                       const nzb_adjoint_march* march, nzb_adjoint** out) {
+  if (!out) return fail("adjoint_create: out is null");
+  *out = nullptr;
+  if (n_buckets < 1 || !meshes || !phys || !buffers || !elem_offset || !march)
+    return fail("adjoint_create: null argument");
+  const nzb_adjoint_march& am = *march;
+  if (am.n_inst < 1 || !am.inst_begin || !am.inst_end || !am.inst_count || !am.elem_norm || !am.status ||
+      !am.iterations || !am.res0 || !am.res || !am.n_running)
+    return fail("adjoint_create: missing march array");
+  if (am.max_iterations < 1 || !(am.tolerance >= 0.0)) return fail("adjoint_create: bad march parameters");
+  if (am.n_inst > 0x7fffffff) return fail("adjoint_create: too many instances");
+  AdjBatch* A = new AdjBatch();
+  for (int b = 0; b < n_buckets; ++b) {
+    if (check_mesh(&meshes[b])) {
+      delete A;
+      return -1;
+    }
+    if (am.n_inst > 1 && (!meshes[b].elem_inst || !meshes[b].inst_status)) {
+      delete A;
+      return fail("adjoint_create: several instances need elem_inst and inst_status");
+    }
+    const nzb_adjoint_buffers& bf = buffers[b];
+    if (!bf.U || !bf.seed || !bf.lam || !bf.Y1 || !bf.Y2 || !bf.f0 || !bf.f1 || !bf.f2 || !bf.dt) {
+      delete A;
+      return fail("adjoint_create: missing bucket buffer");
+    }
+    A->mesh.push_back(meshes[b]);
+    A->phys.push_back(phys[b]);
+    A->buf.push_back(bf);
+    A->offset.push_back(elem_offset[b]);
+  }
+  A->am = am;
+  if (cuda_check(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking), "adjoint stream") ||
+      cuda_check(cudaEventCreateWithFlags(&A->ev_in, cudaEventDisableTiming), "adjoint event") ||
+      cuda_check(cudaEventCreateWithFlags(&A->ev_out, cudaEventDisableTiming), "adjoint event") ||
+      cuda_check(cudaEventCreateWithFlags(&A->fork, cudaEventDisableTiming), "adjoint event")) {
+    nzb_adjoint_destroy(reinterpret_cast<nzb_adjoint*>(A));
+    return -1;
+  }
+  for (int b = 0; b < n_buckets; ++b) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    const int rc = cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "bucket stream") ||
+                   cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "bucket event");
+    if (s) A->bstream.push_back(s);
+    if (ev) A->bdone.push_back(ev);
+    if (rc) {
+      nzb_adjoint_destroy(reinterpret_cast<nzb_adjoint*>(A));
+      return -1;
+    }
+  }
+  *out = reinterpret_cast<nzb_adjoint*>(A);
+  return 0;
+}
+
+int nzb_adjoint_run(nzb_adjoint* adjoint, int n_steps, void* stream) {
+  AdjBatch* A = reinterpret_cast<AdjBatch*>(adjoint);
+  if (!A) return fail("adjoint is null");
+  if (n_steps < 0) return fail("adjoint_run: n_steps must be >= 0");
+  cudaStream_t caller = (cudaStream_t)stream;
+  if (cuda_check(cudaEventRecord(A->ev_in, caller), "event record") ||
+      cuda_check(cudaStreamWaitEvent(A->stream, A->ev_in, 0), "stream wait"))
+    return -1;
+  cudaGraphExec_t ex = nullptr;
+  if (adjoint_graph(*A, n_steps, &ex)) return -1;
+  if (cuda_check(cudaGraphLaunch(ex, A->stream), "graph launch")) return -1;
+  if (cuda_check(cudaEventRecord(A->ev_out, A->stream), "event record") ||
+      cuda_check(cudaStreamWaitEvent(caller, A->ev_out, 0), "stream wait"))
+    return -1;
+  return 0;
+}
+
+int nzb_adjoint_destroy(nzb_adjoint* adjoint) {
+  AdjBatch* A = reinterpret_cast<AdjBatch*>(adjoint);
+  if (!A) return 0;
+  for (auto& kv : A->graphs) cudaGraphExecDestroy(kv.second);
+  if (A->ev_in) cudaEventDestroy(A->ev_in);
+  if (A->ev_out) cudaEventDestroy(A->ev_out);
+  if (A->fork) cudaEventDestroy(A->fork);
+  for (auto ev : A->bdone) cudaEventDestroy(ev);
+  for (auto s : A->bstream) cudaStreamDestroy(s);
+  if (A->stream) cudaStreamDestroy(A->stream);
+  delete A;
   return 0;
 }
 

@@ -133,6 +133,103 @@ def bezier8_sensitivity(x, geom: Geometry) -> np.ndarray:
     return np.where(xi[None, :] <= geom.throat_x, 0.0, out)
 
 
+# ------------------------------------------------------- design variables
+#: Differentiable design variables of a contour (src/geometry/contour.py:55-65),
+#: plus the eight radial offsets of the bezier8 family.
+DESIGN_PARAMETERS = ("area_ratio", "throat_x", "throat_half_height", "inlet_half_height", "theta_initial",
+                     "theta_exit", "bezier_w1", "bezier_w2", "length")
+BEZIER8_PARAMETERS = tuple(f"offset_{k}" for k in range(8))
+
+
+def design_params(geom: Geometry) -> dict:
+    """The design variables as a flat dict, wall angles in radians (src/geometry/contour.py:170-188)."""
+    out = {
+        "area_ratio": float(geom.area_ratio),
+        "throat_x": float(geom.throat_x),
+        "throat_half_height": float(geom.throat_half_height),
+        "inlet_half_height": float(geom.inlet_half_height),
+        "theta_initial": float(geom.theta_initial()),
+        "theta_exit": math.radians(float(geom.theta_exit_deg)),
+        "bezier_w1": float(geom.bezier_w1),
+        "bezier_w2": float(geom.bezier_w2),
+        "length": float(geom.length),
+    }
+    if geom.contour == "bezier8":
+        out.update({f"offset_{k}": float(geom.offsets[k]) for k in range(8)})
+    return out
+
+
+def geometry_with(geom: Geometry, params: dict) -> Geometry:
+    """The geometry at these design variables (src/geometry/contour.py:190-204)."""
+    fields = {}
+    for key, value in params.items():
+        if key == "theta_initial":
+            fields["theta_initial_deg"] = math.degrees(float(value))
+        elif key == "theta_exit":
+            fields["theta_exit_deg"] = math.degrees(float(value))
+        elif key in BEZIER8_PARAMETERS:
+            continue
+        elif key in DESIGN_PARAMETERS:
+            fields[key] = float(value)
+        else:
+            raise ValueError(f"{key!r} is not a design parameter; use {DESIGN_PARAMETERS + BEZIER8_PARAMETERS}")
+    if any(k in params for k in BEZIER8_PARAMETERS):
+        offs = list(geom.offsets)
+        for k in range(8):
+            if f"offset_{k}" in params:
+                offs[k] = float(params[f"offset_{k}"])
+        fields["offsets"] = tuple(offs)
+    return replace(geom, **fields)
+
+
+def wall_from_params(x, params: dict, contour: str, xp=np):
+    """Wall half-height from a design-variable dict, every operation through ``xp``.
+
+    Restates src/geometry/contour.py:264-311 (plus the bezier8 family) so that
+    ``xp = torch`` with tensor parameters gives a differentiable contour; the
+    wall angles are independent variables here, as in the reference's
+    parameterisation.
+    """
+    if contour not in CONTOURS:
+        raise ValueError(f"unknown contour {contour!r}; choose from {CONTOURS}")
+    length = params.get("length", 1.0)
+    xi = xp.asarray(x) / length
+    y_th = params["throat_half_height"]
+    y_in = params["inlet_half_height"]
+    y_ex = y_th * params["area_ratio"]
+    x_th = params["throat_x"]
+    y_conv = _hermite(xp.clip(xi / x_th, 0.0, 1.0), y_in, y_th, 0.0, 0.0)
+    span = 1.0 - x_th
+    s = xp.clip((xi - x_th) / span, 0.0, 1.0)
+    dx_ds = span * length
+    if contour == "conical":
+        y_div = y_th + (y_ex - y_th) * s
+    elif contour in ("bell", "smooth", "moc"):
+        y_div = _hermite(s, y_th, y_ex, xp.tan(xp.asarray(params["theta_initial"])) * dx_ds,
+                         xp.tan(xp.asarray(params["theta_exit"])) * dx_ds)
+    elif contour == "bezier":
+        c1 = y_th + params["bezier_w1"] * (y_ex - y_th)
+        c2 = y_th + params["bezier_w2"] * (y_ex - y_th)
+        u = 1.0 - s
+        y_div = u**3 * y_th + 3.0 * u**2 * s * c1 + 3.0 * u * s**2 * c2 + s**3 * y_ex
+    else:
+        base = _hermite(s, y_th, y_ex, 0.0, xp.tan(xp.asarray(params["theta_exit"])) * dx_ds)
+        bump = sum(_bernstein(BEZIER8_DEGREE, k + 1, s) * params[f"offset_{k}"] for k in range(8))
+        y_div = base + y_th * bump
+    return xp.where(xi <= x_th, y_conv, y_div)
+
+
+def node_coords_from_params(x_frac, r_frac, params: dict, contour: str, xp=np):
+    """Node coordinates ``(x, r y_wall(x))`` of the frozen logical grid (src/geometry/mesh.py:467-490)."""
+    length = params.get("length", 1.0)
+    x = xp.asarray(x_frac) * length
+    yw = wall_from_params(x, params, contour, xp)
+    nr, nx = len(r_frac), len(x_frac)
+    xx = xp.broadcast_to(x[None, :], (nr, nx))
+    yy = xp.asarray(r_frac)[:, None] * yw[None, :]
+    return xp.stack([xx.reshape(-1), yy.reshape(-1)], -1)
+
+
 # ---------------------------------------------------------------- node grids
 def clustered_distribution(n_intervals, x_throat, strength, width):
     if strength < 1.0:

@@ -27,6 +27,10 @@
  *                                 src/backends/_numba_kernels.py:789-850
  *   nzb_norm                     Backend.norm              src/backends/numba_backend.py:178-181
  *   nzb_solver_*                 NumbaBackend.run          src/backends/numba_backend.py:283-337
+ *   nzb_vjp, nzb_adjoint_*       jax.vjp of assembly.residual and the RK4 march of
+ *                                 DifferentiableCase.adjoint_solve src/sensitivity.py:289-383
+ *   nzb_vjp_coords               jax.vjp of the residual w.r.t. the design variables
+ *                                 through the node coordinates     src/sensitivity.py:453-458
  */
 #ifndef NOZZLE_B200_H
 #define NOZZLE_B200_H
@@ -242,6 +246,99 @@ int nzb_batch_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics* p
  * single step that sets res0), then run the device check. */
 int nzb_batch_run(nzb_batch* batch, int n_steps, int first, void* stream);
 int nzb_batch_destroy(nzb_batch* batch);
+
+/* ---- discrete adjoint ----------------------------------------------------------
+ * Products with the transposed Jacobians of the UNFOLDED residual R (M dU/dt =
+ * -R, src/spatial/assembly.py:153-157) and the adjoint pseudo-time march of
+ * DifferentiableCase.adjoint_solve (src/sensitivity.py:289-383):
+ *   dlam/dtau = -M^-1 ((dR/dU)^T lam - seed),  classical RK4, frozen local step,
+ * which replace the reference's jax.vjp of assembly.residual.  The flux
+ * Jacobians are exact (forward-mode dual numbers through the same flux code);
+ * the limiter is not part of the linearisation, as in the reference.
+ *
+ * nzb_vjp modes:
+ *   VJP     out = (dR/dU)^T lam
+ *   DEFECT  out = (dR/dU)^T lam - seed (out nullable); norm_partial[block] and
+ *           elem_norm[e] (both nullable) receive sums of its squares
+ *   RATE    out = -M^-1 ((dR/dU)^T lam - seed)
+ *   RK4     stage k of lam_new = lam0 + dt/6 (f0 + 2 f1 + 2 f2 + f3), with
+ *           f_k = RATE at lam (this stage's input): stages 0..2 store f_k and
+ *           write the next input lam0 + c dt f_k to out (c = 1/2, 1/2, 1);
+ *           stage 3 overwrites lam0 with lam_new.  lam must not alias out
+ *           (stages 0-2) or lam0 (stage 3). */
+enum { NZB_ADJ_VJP = 0, NZB_ADJ_DEFECT = 1, NZB_ADJ_RATE = 2, NZB_ADJ_RK4 = 3 };
+typedef struct {
+  int32_t mode;
+  int32_t stage;
+  const double* U;    /* (4, NP, E) linearisation state */
+  const double* lam;  /* (4, NP, E) */
+  const double* seed; /* (4, NP, E) dJ/dU */
+  double* out;
+  double* lam0;
+  const double* dt;   /* (E) frozen local step */
+  double* f0;
+  double* f1;
+  double* f2;
+  double* norm_partial; /* nzb_element_blocks(mesh) doubles */
+  double* elem_norm;    /* (E) */
+} nzb_adjoint_args;
+int nzb_vjp(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_adjoint_args* args, void* stream);
+
+/* (dR/dX)^T lam per element vertex and (dR/dp_back)^T lam per element, the
+ * products DifferentiableCase.value_and_gradient takes through the node
+ * coordinates (src/sensitivity.py:453-458, src/spatial/operators.py:207-303).
+ * verts (2 NV, E): vertex x then y coordinates (NV = 3 triangles, 4 quads);
+ * dgs (16 doubles, row f, column v): the face tangent dX/dsigma of face f is
+ * sum_v dgs[4 f + v] X_v (the reference's dgeom_dsigma_face, straight edges);
+ * gvert (2 NV, E) out; gpb (E) out, nullable.  Summing gvert over the
+ * elements that share a node gives d(lam . R)/d(node). */
+int nzb_vjp_coords(const nzb_mesh* mesh, const nzb_physics* phys, const double* U, const double* lam,
+                   const double* verts, const double* dgs, double* gvert, double* gpb, void* stream);
+
+/* dt_e = coefficient * 2 A_e / max(wave_e, 1e-10): local_time_step
+ * (src/timestepping/step.py:171-183). */
+int nzb_local_dt(const nzb_mesh* mesh, const double* wave, double coefficient, double* dt, void* stream);
+
+/* The adjoint march over many independent instances (buckets as for
+ * nzb_batch_*; a single solve is one bucket with one instance, elem_inst
+ * nullable).  Each bucket: U (converged state), seed, lam (in/out), scratch
+ * Y1, Y2, f0, f1, f2 (all (4, NP, E)) and dt (E).  nzb_adjoint_run(n_steps =
+ * 0) takes the defect of the current lam as res0 (with lam = 0: rms(seed));
+ * n_steps > 0 advances every running instance n_steps RK4 steps, then
+ * measures res = rms((dR/dU)^T lam - seed) and sets status: 1 converged (res
+ * <= tolerance * res0, or res0 = 0), 2 non-finite, 5 iteration cap. */
+typedef struct {
+  const double* U;
+  const double* seed;
+  double* lam;
+  double* Y1;
+  double* Y2;
+  double* f0;
+  double* f1;
+  double* f2;
+  const double* dt;
+} nzb_adjoint_buffers;
+typedef struct {
+  int64_t n_inst;
+  const int64_t* inst_begin; /* (n_inst) first element, global numbering */
+  const int64_t* inst_end;
+  const double* inst_count;  /* (n_inst) 4 * NP * E_i */
+  double* elem_norm;         /* (sum E) scratch */
+  int32_t* status;           /* (n_inst) 0 running, 1 converged, 2 non-finite, 5 iteration cap */
+  int32_t* iterations;       /* (n_inst) */
+  double* res0;              /* (n_inst) */
+  double* res;               /* (n_inst) */
+  int32_t* n_running;        /* (1) */
+  double tolerance;
+  int32_t max_iterations;
+  int32_t reserved;
+} nzb_adjoint_march;
+typedef struct nzb_adjoint nzb_adjoint;
+int nzb_adjoint_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics* phys,
+                       const nzb_adjoint_buffers* buffers, const int64_t* elem_offset,
+                       const nzb_adjoint_march* march, nzb_adjoint** out);
+int nzb_adjoint_run(nzb_adjoint* adjoint, int n_steps, void* stream);
+int nzb_adjoint_destroy(nzb_adjoint* adjoint);
 
 const char* nzb_last_error(void);
 int nzb_version(void);

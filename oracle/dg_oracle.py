@@ -40,6 +40,18 @@ INFLOW, OUTFLOW, WALL, AXIS = 1, 2, 3, 4
 
 
 # ---------------------------------------------------------------- physics
+def _abs(x):
+    """|x|.  For a complex-step argument x + i h (h tiny), x times the sign of
+    its real part: analytic, so the imaginary part carries the derivative of
+    |x| (the modulus would drop it).  Real arguments go to numpy.abs."""
+    if np.iscomplexobj(x):
+        return np.where(np.real(x) < 0.0, -x, x)
+    return np.abs(x)
+
+
+def _sign(x):
+    return np.sign(np.real(x))
+
 def primitives(U, g):
     rho = np.maximum(U[..., 0], FLOOR)
     vx = U[..., 1] / rho
@@ -73,7 +85,7 @@ def roe(UL, UR, nx, ny, g, efix):
     q2 = u * u + v * v
     c = np.sqrt(np.maximum((g - 1.0) * (H - 0.5 * q2), FLOOR))
     vn = u * nx + v * ny
-    l1, l2, l3 = np.abs(vn + c), np.abs(vn - c), np.abs(vn)
+    l1, l2, l3 = _abs(vn + c), _abs(vn - c), _abs(vn)
     smax = np.maximum(l1, l2)
     eps = efix * c
     with np.errstate(divide="ignore", invalid="ignore"):
@@ -105,17 +117,17 @@ def hllc(UL, UR, nx, ny, g, low_mach=0.0):
     SL = np.minimum(vnL - aL, vt - at)
     SR = np.maximum(vnR + aR, vt + at)
     if low_mach > 0.0:
-        mach = np.maximum(np.abs(vnL) / aL, np.abs(vnR) / aR)
+        mach = np.maximum(_abs(vnL) / aL, _abs(vnR) / aR)
         phi = np.minimum(1.0, mach / low_mach)
         bL, bR = np.minimum(vnL, vt), np.maximum(vnR, vt)
         SL = bL - phi * (bL - SL)
         SR = bR + phi * (SR - bR)
     mL, mR = rL * (SL - vnL), rR * (SR - vnR)
-    dm = np.where(np.abs(mR - mL) > FLOOR, mR - mL, FLOOR)
+    dm = np.where(_abs(mR - mL) > FLOOR, mR - mL, FLOOR)
     SM = (rR * vnR * (SR - vnR) - rL * vnL * (SL - vnL) + pL - pR) / dm
 
     def guard(x):
-        return np.where(np.abs(x) > FLOOR, x, FLOOR)
+        return np.where(_abs(x) > FLOOR, x, FLOOR)
 
     def star(U, r, u_, v_, p, vn, S):
         fac = (S - vn) / guard(S - SM)
@@ -128,7 +140,7 @@ def hllc(UL, UR, nx, ny, g, low_mach=0.0):
     FsL = FL + SL[..., None] * (star(UL, rL, uL, vL, pL, vnL, SL) - UL)
     FsR = FR + SR[..., None] * (star(UR, rR, uR, vR, pR, vnR, SR) - UR)
     F = np.where((SL >= 0.0)[..., None], FL, np.where((SR <= 0.0)[..., None], FR, np.where((SM >= 0.0)[..., None], FsL, FsR)))
-    return F, np.maximum(np.abs(SL), np.abs(SR))
+    return F, np.maximum(_abs(SL), _abs(SR))
 
 
 _B, _A, _KP, _KU = 0.125, 0.1875, 0.4, 0.2
@@ -148,18 +160,18 @@ def ausmup(UL, UR, nx, ny, g):
 
     pL2, mL2 = m2(mL)
     pR2, mR2 = m2(mR)
-    m4p = np.where(np.abs(mL) >= 1.0, 0.5 * (mL + np.abs(mL)), pL2 * (1.0 - 16.0 * _B * mL2))
-    m4m = np.where(np.abs(mR) >= 1.0, 0.5 * (mR - np.abs(mR)), mR2 * (1.0 + 16.0 * _B * pR2))
+    m4p = np.where(_abs(mL) >= 1.0, 0.5 * (mL + _abs(mL)), pL2 * (1.0 - 16.0 * _B * mL2))
+    m4m = np.where(_abs(mR) >= 1.0, 0.5 * (mR - _abs(mR)), mR2 * (1.0 + 16.0 * _B * pR2))
     uh = ah * (m4p + m4m) + _KP * np.maximum(1.0 - mb2, 0.0) * (pL - pR) / (rh * ah)
-    p5p = np.where(np.abs(mL) >= 1.0, 0.5 * (1.0 + np.sign(mL)), pL2 * ((2.0 - mL) - 16.0 * _A * mL * mL2))
-    p5m = np.where(np.abs(mR) >= 1.0, 0.5 * (1.0 - np.sign(mR)), mR2 * ((-2.0 - mR) + 16.0 * _A * mR * pR2))
+    p5p = np.where(_abs(mL) >= 1.0, 0.5 * (1.0 + _sign(mL)), pL2 * ((2.0 - mL) - 16.0 * _A * mL * mL2))
+    p5m = np.where(_abs(mR) >= 1.0, 0.5 * (1.0 - _sign(mR)), mR2 * ((-2.0 - mR) + 16.0 * _A * mR * pR2))
     ph = p5p * pL + p5m * pR + _KU * p5p * p5m * rh * ah * (vnL - vnR)
     PsiL = np.stack([rL, rL * uL, rL * vL, UL[..., 3] + pL], -1)
     PsiR = np.stack([rR, rR * uR, rR * vR, UR[..., 3] + pR], -1)
-    F = 0.5 * uh[..., None] * (PsiL + PsiR) - 0.5 * np.abs(uh)[..., None] * (PsiR - PsiL)
+    F = 0.5 * uh[..., None] * (PsiL + PsiR) - 0.5 * _abs(uh)[..., None] * (PsiR - PsiL)
     z = np.zeros_like(ph)
     F = F + ph[..., None] * np.stack([z, nx + z, ny + z, z], -1)
-    return F, np.maximum(np.abs(vnL) + aL, np.abs(vnR) + aR)
+    return F, np.maximum(_abs(vnL) + aL, _abs(vnR) + aR)
 
 
 def wall(U, nx, ny, g):
@@ -184,7 +196,7 @@ def inflow(U, nx, ny, g, Tt, pt, Rgas, alpha):
     qa = 0.5 * (g - 1.0) * beta - nd * nd
     qb = -4.0 * nd / (g - 1.0)
     qc = beta - (2.0 / (g - 1.0)) ** 2
-    qa = np.where(np.abs(qa) < 1e-12, np.where(qa >= 0, 1e-12, -1e-12), qa)
+    qa = np.where(_abs(qa) < 1e-12, np.where(qa >= 0, 1e-12, -1e-12), qa)
     sq = np.sqrt(np.maximum(qb * qb - 4.0 * qa * qc, 0.0))
     r1, r2 = (-qb + sq) / (2.0 * qa), (-qb - sq) / (2.0 * qa)
     M = np.minimum(np.where(r1 >= 0.0, r1, 1e30), np.where(r2 >= 0.0, r2, 1e30))
@@ -196,7 +208,7 @@ def inflow(U, nx, ny, g, Tt, pt, Rgas, alpha):
     Hb = at2 / (g - 1.0)
     vnb = vxb * nx + vyb * ny
     F = np.stack([rhob * vnb, rhob * vxb * vnb + pb * nx, rhob * vyb * vnb + pb * ny, rhob * Hb * vnb], -1)
-    return F, np.abs(vnb) + ab
+    return F, _abs(vnb) + ab
 
 
 def outflow(U, nx, ny, g, p_back, rho_t=0.0, p_t=1.0, band=0.05):
@@ -223,7 +235,7 @@ def outflow(U, nx, ny, g, p_back, rho_t=0.0, p_t=1.0, band=0.05):
     Ub = np.where((vn / a >= 1.0)[..., None], U, Us)
     F = normal_flux(Ub, nx, ny, g)
     ro, uo, vo, po, _ = primitives(Ub, g)
-    return F, np.abs(uo * nx + vo * ny) + np.sqrt(g * po / ro)
+    return F, _abs(uo * nx + vo * ny) + np.sqrt(g * po / ro)
 
 
 def interface(flow, UL, UR, nx, ny):
@@ -255,8 +267,8 @@ def edge_fluxes(U, ops, flow):
     F_i, s_i = interface(flow, UL, UR, nrm[:ni, :, 0], nrm[:ni, :, 1])
     Ub = np.einsum("kiq,kis->kqs", pf[0][ed.bedge_face], U[ed.bedge_elem])
     nb = nrm[ni:]
-    Fb = np.zeros_like(Ub)
-    sb = np.zeros(Ub.shape[:2])
+    Fb = np.zeros(Ub.shape, dtype=np.result_type(Ub, nb))
+    sb = np.zeros(Ub.shape[:2], dtype=Fb.dtype)
     g = flow.gamma
     for tag, sl in ed.tag_slices.items():
         u, nx, ny = Ub[sl], nb[sl, :, 0], nb[sl, :, 1]
@@ -272,8 +284,10 @@ def edge_fluxes(U, ops, flow):
 
 
 def residual(U, ops, flow):
-    """``(R, wave)`` with ``M dU/dt = -R``."""
-    U = np.asarray(U, float)
+    """``(R, wave)`` with ``M dU/dt = -R``.  Complex U (a complex step) is kept complex."""
+    U = np.asarray(U)
+    if not np.iscomplexobj(U):
+        U = U.astype(float)
     F, speed = edge_fluxes(U, ops, flow)
     uq = np.einsum("iq,eis->eqs", ops.ref.phi_vol, U)
     Fx, Fy = euler_flux(uq, flow.gamma)
@@ -413,3 +427,118 @@ class Stepper:
             for _ in range(n):
                 U, res = self.step(U)
         return U, res
+
+
+# ---------------------------------------------------------------- adjoint
+# The reference takes its adjoint's derivatives from JAX (src/sensitivity.py:
+# 289-460).  Here they come from complex steps through the restatement above:
+# f(x + i h) = f(x) + i h f'(x) + O(h^2) for an analytic f, so Im f / h is the
+# derivative to round-off with h = 1e-30 (no cancellation, unlike a finite
+# difference).  Branches compare real parts, as the reference's do.
+H_CS = 1e-30
+
+
+class _Ops:
+    pass
+
+
+def operators_at(ops, X):
+    """The operator fields ``residual`` reads, rebuilt at node coordinates X (real or complex).
+
+    Restates src/spatial/operators.py:238-303 for straight-sided (Q = 1)
+    elements: metrics from the vertex map, w det (dphi/dx, dphi/dy), the mass
+    matrix and its inverse, the owner's edge tangent, |dX/dsigma|, the normal
+    (t_y, -t_x)/|t| and the edge length.
+    """
+    rd, topo = ops.ref, ops.topology
+    X = np.asarray(X)
+    Xe = X[topo.elem_nodes]
+    x_xi, x_eta = Xe[:, :, 0] @ rd.dgeom_dxi_vol, Xe[:, :, 0] @ rd.dgeom_deta_vol
+    y_xi, y_eta = Xe[:, :, 1] @ rd.dgeom_dxi_vol, Xe[:, :, 1] @ rd.dgeom_deta_vol
+    det = x_xi * y_eta - x_eta * y_xi
+    inv = 1.0 / det
+    xi_x, xi_y, eta_x, eta_y = y_eta * inv, -x_eta * inv, -y_xi * inv, x_xi * inv
+    wdet = rd.w_vol[None, :] * det
+    out = _Ops()
+    out.ref, out.topology = rd, topo
+    out.grad_x = wdet[:, None, :] * (rd.dphi_dxi_vol[None] * xi_x[:, None, :] + rd.dphi_deta_vol[None] * eta_x[:, None, :])
+    out.grad_y = wdet[:, None, :] * (rd.dphi_dxi_vol[None] * xi_y[:, None, :] + rd.dphi_deta_vol[None] * eta_y[:, None, :])
+    out.inv_mass = np.linalg.inv(np.einsum("iq,jq,eq->eij", rd.phi_vol, rd.phi_vol, wdet))
+    out.elem_area = wdet.sum(axis=1)
+    ed = topo.edges
+    owner_e = np.concatenate([ed.iedge_elem[:, 0], ed.bedge_elem])
+    owner_f = np.concatenate([ed.iedge_face[:, 0], ed.bedge_face])
+    t = np.einsum("enq,end->eqd", np.asarray(rd.dgeom_dsigma_face)[owner_f], Xe[owner_e])
+    jac = np.sqrt(t[..., 0] ** 2 + t[..., 1] ** 2)
+    out.edge_jac = jac
+    out.edge_normal = np.stack([t[..., 1], -t[..., 0]], -1) / jac[..., None]
+    out.edge_length = (jac * rd.w_face[None, :]).sum(axis=1)
+    out.face_edge = ops.face_edge
+    out.face_sign = ops.face_sign
+    out.n_elem = ops.n_elem
+    return out
+
+
+def state_jacobian(U, ops, flow):
+    """dR/dU as a dense (n, n) matrix over the flattened (E, NP, 4) state, by complex steps."""
+    U = np.asarray(U, float)
+    n = U.size
+    J = np.empty((n, n))
+    for k in range(n):
+        Uc = U.astype(complex).ravel()
+        Uc[k] += 1j * H_CS
+        J[:, k] = residual(Uc.reshape(U.shape), ops, flow)[0].imag.ravel() / H_CS
+    return J
+
+
+def state_vjp(U, lam, ops, flow, J=None):
+    """(dR/dU)^T lam in the (E, NP, 4) layout."""
+    J = state_jacobian(U, ops, flow) if J is None else J
+    return (J.T @ np.asarray(lam, float).ravel()).reshape(np.shape(U))
+
+
+def coord_vjp(U, lam, ops, flow):
+    """(dR/dX)^T lam as an (N_nodes, 2) array, by one complex step per node coordinate."""
+    X = np.asarray(ops.node_coords, float)
+    lam = np.asarray(lam, float)
+    g = np.zeros_like(X)
+    Uc = np.asarray(U, float).astype(complex)
+    for a in range(X.shape[0]):
+        for d in range(2):
+            Xc = X.astype(complex)
+            Xc[a, d] += 1j * H_CS
+            R = residual(Uc, operators_at(ops, Xc), flow)[0]
+            g[a, d] = float(np.sum(lam * R.imag)) / H_CS
+    return g
+
+
+def back_pressure_vjp(U, lam, ops, flow):
+    """(dR/dp_back)^T lam by a complex step on the back pressure."""
+    import dataclasses
+
+    fc = dataclasses.replace(flow, back_pressure_ratio=flow.back_pressure_ratio + 1j * H_CS / flow.total_pressure)
+    R = residual(np.asarray(U, float).astype(complex), ops, fc)[0]
+    return float(np.sum(np.asarray(lam, float) * R.imag)) / H_CS
+
+
+def adjoint_march(U, seed, ops, flow, cfl, n_steps, J=None):
+    """n_steps of the adjoint pseudo-time march from lam = 0 (src/sensitivity.py:318-358):
+    dlam/dtau = -M^-1 ((dR/dU)^T lam - seed), classical RK4, dt frozen from the
+    converged state with the SSP-RK3 coefficient at cfl."""
+    U = np.asarray(U, float)
+    J = state_jacobian(U, ops, flow) if J is None else J
+    seed = np.asarray(seed, float)
+    _, wave = residual(U, ops, flow)
+    dt = time_step(wave, ops, ops.ref.order, cfl, "ssprk3")[:, None, None]
+
+    def rate(lam):
+        return -inverse_mass(state_vjp(U, lam, ops, flow, J) - seed, ops)
+
+    lam = np.zeros_like(seed)
+    for _ in range(n_steps):
+        f0 = rate(lam)
+        f1 = rate(lam + 0.5 * dt * f0)
+        f2 = rate(lam + 0.5 * dt * f1)
+        f3 = rate(lam + dt * f2)
+        lam = lam + dt / 6.0 * (f0 + 2.0 * f1 + 2.0 * f2 + f3)
+    return lam

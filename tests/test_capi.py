@@ -59,6 +59,9 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(capi.Physics) == 3 * 8 + 8 + 9 * 8 + 4 * 8 + 8 + 4 * 8
     assert ctypes.sizeof(capi.StageArgs) == 8 * 8 + 3 * 8 + 8
     assert ctypes.sizeof(capi.BatchMarch) == 8 + 12 * 8 + 2 * 8 + 2 * 4
+    assert ctypes.sizeof(capi.AdjointArgs) == 8 + 11 * 8
+    assert ctypes.sizeof(capi.AdjointBuffers) == 9 * 8
+    assert ctypes.sizeof(capi.AdjointMarch) == 8 + 9 * 8 + 8 + 2 * 4
 
 
 def test_lebesgue_constant_bounds_probe_values():
