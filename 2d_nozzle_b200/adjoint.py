@@ -75,7 +75,7 @@ class AdjointModel:
         self.device = self.mesh.device
         self.E, self.NP, self.NV = self.mesh.E, self.mesh.np_, self.mesh.nf
         self.phys = physics_struct(flow, opts, ops.ref)
-        self.dgs = torch.as_tensor(face_tangent_table(ops.ref).ravel(), device=self.device)
+        self.dgs = np.ascontiguousarray(face_tangent_table(ops.ref).ravel())  # host: passed by value to the kernel
         self.elem_nodes = np.ascontiguousarray(np.asarray(ops.topology.elem_nodes)[:, : self.NV])
         self.elem_nodes_t = torch.as_tensor(self.elem_nodes, device=self.device)
         self.X0 = torch.as_tensor(np.asarray(ops.node_coords, float), device=self.device)
@@ -161,7 +161,7 @@ class AdjointModel:
         gpb = torch.empty(self.E, dtype=torch.float64, device=self.device)
         verts = self.verts(X)
         capi.check(self.lib.nzb_vjp_coords(C.byref(self.mesh_at(X).c), C.byref(ph), U_soa.data_ptr(),
-                                           lam_soa.data_ptr(), verts.data_ptr(), self.dgs.data_ptr(), gvert.data_ptr(),
+                                           lam_soa.data_ptr(), verts.data_ptr(), self.dgs.ctypes.data, gvert.data_ptr(),
                                            gpb.data_ptr(), self.stream), "nzb_vjp_coords")
         return gvert.reshape(2, self.NV, self.E), gpb
 

@@ -2,9 +2,11 @@
 
     python -m <package>.build            (or: python 2d_nozzle_b200/build.py)
 
-The library is a single translation unit (``csrc/capi.cu``) compiled by nvcc
-for ``sm_100a`` only, with ``-lineinfo`` for profiler source mapping.  It links
-the CUDA runtime statically, so loading it needs nothing but the driver.
+Every ``csrc/*.cu`` translation unit (the C ABI with the forward kernels, and
+the adjoint kernels per element kind) is compiled by nvcc for ``sm_100a``
+only, with ``-lineinfo`` for profiler source mapping, in parallel; the objects
+are linked into one library with the CUDA runtime linked statically, so
+loading it needs nothing but the driver.
 """
 
 from __future__ import annotations
@@ -15,7 +17,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "capi.cu")
+CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libnozzle_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -42,39 +44,45 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
+def units() -> list[str]:
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    tmp = LIB + f".tmp{os.getpid()}"
-    cmd = [
-        nvcc(),
-        *ARCH,
-        "-O3",
-        "-lineinfo",
-        "-std=c++17",
-        "--expt-relaxed-constexpr",
-        "-shared",
-        "-Xcompiler",
-        "-fPIC",
-        "-cudart",
-        "static",
-        "-I",
-        os.path.join(ROOT, "include"),
-        "-I",
-        os.path.join(HERE, "csrc"),
-        SRC,
-        "-o",
-        tmp,
-    ]
+    tag = f"tmp{os.getpid()}"
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+             "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stderr[-6000:]}")
-    if verbose:
-        sys.stderr.write(res.stderr)
-    os.replace(tmp, LIB)
+        flags.insert(0, "-Xptxas=-v")
+    objs, procs = [], []
+    for src in units():
+        obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + f".{tag}.o")
+        objs.append(obj)
+        procs.append((src, subprocess.Popen([nvcc(), *flags, "-c", src, "-o", obj], stdout=subprocess.PIPE,
+                                            stderr=subprocess.PIPE, text=True)))
+    errors = []
+    for src, pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            errors.append(f"{os.path.basename(src)}: nvcc failed ({pr.returncode}):\n{err[-6000:]}")
+        elif verbose:
+            sys.stderr.write(err)
+    try:
+        if errors:
+            raise RuntimeError("\n".join(errors))
+        tmp = LIB + f".{tag}"
+        res = subprocess.run([nvcc(), *ARCH, "-shared", "-cudart", "static", *objs, "-o", tmp], capture_output=True,
+                             text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed ({res.returncode}):\n{res.stderr[-6000:]}")
+        os.replace(tmp, LIB)
+    finally:
+        for o in objs:
+            if os.path.exists(o):
+                os.remove(o)
     return LIB
 
 

@@ -1,0 +1,46 @@
+// adjoint_tri.cu -- the adjoint kernels for triangles, p = 0..3.
+#include "adjoint_dispatch.cuh"
+
+namespace nzb {
+namespace {
+
+template <int K, int P, bool AFF>
+cudaError_t launch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
+  const int64_t nb = (m.n_elem + Launch<K, P>::NT - 1) / Launch<K, P>::NT;
+  k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  return cudaGetLastError();
+}
+
+template <int K, int P>
+cudaError_t launch_coords(const nzb_mesh& m, const nzb_physics& ph, const CoordWork& w, cudaStream_t st) {
+  k_vjp_coords<K, P><<<(unsigned)((m.n_elem + 127) / 128), 128, 0, st>>>(m, ph, w);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t vjp_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
+  switch (m.order) {
+    case 0: return m.affine ? launch_vjp<0, 0, true>(m, ph, w, st) : launch_vjp<0, 0, false>(m, ph, w, st);
+    case 1: return m.affine ? launch_vjp<0, 1, true>(m, ph, w, st) : launch_vjp<0, 1, false>(m, ph, w, st);
+    case 2: return m.affine ? launch_vjp<0, 2, true>(m, ph, w, st) : launch_vjp<0, 2, false>(m, ph, w, st);
+    case 3: return m.affine ? launch_vjp<0, 3, true>(m, ph, w, st) : launch_vjp<0, 3, false>(m, ph, w, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t vjp_coords_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const CoordWork& w, cudaStream_t st) {
+  switch (m.order) {
+    case 0: return launch_coords<0, 0>(m, ph, w, st);
+    case 1: return launch_coords<0, 1>(m, ph, w, st);
+    case 2: return launch_coords<0, 2>(m, ph, w, st);
+    case 3: return launch_coords<0, 3>(m, ph, w, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t upload_tables_tri(const double* src, size_t count, size_t offset) {
+  return cudaMemcpyToSymbol(c_tab, src, sizeof(double) * count, sizeof(double) * offset);
+}
+
+}  // namespace nzb

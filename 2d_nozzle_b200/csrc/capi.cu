@@ -14,7 +14,7 @@
 #include <utility>
 #include <vector>
 
-#include "adjoint.cuh"
+#include "adjoint_dispatch.cuh"
 #include "element.cuh"
 #include "nozzle_b200.h"
 
@@ -434,50 +434,17 @@ static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
 }
 
 // ---- adjoint ------------------------------------------------------------------
-template <int K, int P, bool AFF>
-static int launch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
-  const int64_t nb = element_blocks(m);
-  if (nb > 0x7fffffff) return fail("too many elements for one launch");
-  k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
-  return launch_check("vjp kernel launch");
-}
-
+// The adjoint kernels live in adjoint_tri.cu / adjoint_quad.cu.
 static int dispatch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
-#define NZB_CASE(K, P)                                                       \
-  if (m.kind == K && m.order == P) {                                         \
-    if (K == 0 && m.affine) return launch_vjp<K, P, (K == 0)>(m, ph, w, st); \
-    return launch_vjp<K, P, false>(m, ph, w, st);                            \
-  }
-  NZB_CASE(0, 0)
-  NZB_CASE(0, 1)
-  NZB_CASE(0, 2)
-  NZB_CASE(0, 3)
-  NZB_CASE(1, 0)
-  NZB_CASE(1, 1)
-  NZB_CASE(1, 2)
-  NZB_CASE(1, 3)
-#undef NZB_CASE
-  return fail("unsupported kind/order");
+  if (element_blocks(m) > 0x7fffffff) return fail("too many elements for one launch");
+  const cudaError_t e = m.kind == NZB_TRI ? vjp_launch_tri(m, ph, w, st) : vjp_launch_quad(m, ph, w, st);
+  return cuda_check(e, "vjp kernel launch");
 }
 
 static int dispatch_vjp_coords(const nzb_mesh& m, const nzb_physics& ph, const CoordWork& w, cudaStream_t st) {
-  const int64_t nb = (m.n_elem + 127) / 128;
-  if (nb > 0x7fffffff) return fail("too many elements for one launch");
-#define NZB_CASE(K, P)                                          \
-  if (m.kind == K && m.order == P) {                            \
-    k_vjp_coords<K, P><<<(unsigned)nb, 128, 0, st>>>(m, ph, w); \
-    return launch_check("vjp_coords kernel launch");            \
-  }
-  NZB_CASE(0, 0)
-  NZB_CASE(0, 1)
-  NZB_CASE(0, 2)
-  NZB_CASE(0, 3)
-  NZB_CASE(1, 0)
-  NZB_CASE(1, 1)
-  NZB_CASE(1, 2)
-  NZB_CASE(1, 3)
-#undef NZB_CASE
-  return fail("unsupported kind/order");
+  if ((m.n_elem + 127) / 128 > 0x7fffffff) return fail("too many elements for one launch");
+  const cudaError_t e = m.kind == NZB_TRI ? vjp_coords_launch_tri(m, ph, w, st) : vjp_coords_launch_quad(m, ph, w, st);
+  return cuda_check(e, "vjp_coords kernel launch");
 }
 
 __global__ void k_local_dt(const double* __restrict__ area, const double* __restrict__ wave, int64_t E, double coef,
@@ -679,8 +646,11 @@ int nzb_upload_tables(int kind, int order, const double* tables, int64_t n) {
   if (nzb_table_size(kind, order) < 0) return fail("unsupported kind/order");
   if (n != slot_size(kind, order)) return fail("table size mismatch");
   if (!tables) return fail("tables is null");
-  if (cuda_check(cudaMemcpyToSymbol(c_tab, tables, sizeof(double) * n, sizeof(double) * slot_offset(kind, order)),
-                 "table upload"))
+  // every translation unit holds its own copy of the tables
+  const size_t off = (size_t)slot_offset(kind, order);
+  if (cuda_check(cudaMemcpyToSymbol(c_tab, tables, sizeof(double) * n, sizeof(double) * off), "table upload") ||
+      cuda_check(upload_tables_tri(tables, (size_t)n, off), "table upload (adjoint, triangles)") ||
+      cuda_check(upload_tables_quad(tables, (size_t)n, off), "table upload (adjoint, quadrilaterals)"))
     return -1;
   int dev = 0;
   cudaGetDevice(&dev);

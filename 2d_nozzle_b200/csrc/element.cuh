@@ -30,7 +30,8 @@
 
 namespace nzb {
 
-__constant__ double c_tab[TABLE_DOUBLES];
+// one copy per translation unit (each is uploaded by nzb_upload_tables)
+static __constant__ double c_tab[TABLE_DOUBLES];
 
 enum { OP_RESIDUAL = 0, OP_RATE = 1, OP_STAGE = 2, OP_LIMIT = 3 };
 

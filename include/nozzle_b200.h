@@ -288,8 +288,9 @@ int nzb_vjp(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_adjoint_arg
  * products DifferentiableCase.value_and_gradient takes through the node
  * coordinates (src/sensitivity.py:453-458, src/spatial/operators.py:207-303).
  * verts (2 NV, E): vertex x then y coordinates (NV = 3 triangles, 4 quads);
- * dgs (16 doubles, row f, column v): the face tangent dX/dsigma of face f is
- * sum_v dgs[4 f + v] X_v (the reference's dgeom_dsigma_face, straight edges);
+ * dgs (16 doubles in HOST memory, row f, column v): the face tangent dX/dsigma
+ * of face f is sum_v dgs[4 f + v] X_v (the reference's dgeom_dsigma_face,
+ * straight edges); it is copied into the kernel's parameters;
  * gvert (2 NV, E) out; gpb (E) out, nullable.  Summing gvert over the
  * elements that share a node gives d(lam . R)/d(node). */
 int nzb_vjp_coords(const nzb_mesh* mesh, const nzb_physics* phys, const double* U, const double* lam,
