@@ -182,6 +182,12 @@ def geometry_with(geom: Geometry, params: dict) -> Geometry:
     return replace(geom, **fields)
 
 
+def _as_array(a, xp):
+    # arrays are used as they are: torch.asarray would hand a tensor back with
+    # requires_grad switched off, cutting the gradient through it
+    return a if hasattr(a, "shape") else xp.asarray(a)
+
+
 def wall_from_params(x, params: dict, contour: str, xp=np):
     """Wall half-height from a design-variable dict, every operation through ``xp``.
 
@@ -193,7 +199,7 @@ def wall_from_params(x, params: dict, contour: str, xp=np):
     if contour not in CONTOURS:
         raise ValueError(f"unknown contour {contour!r}; choose from {CONTOURS}")
     length = params.get("length", 1.0)
-    xi = xp.asarray(x) / length
+    xi = _as_array(x, xp) / length
     y_th = params["throat_half_height"]
     y_in = params["inlet_half_height"]
     y_ex = y_th * params["area_ratio"]
@@ -205,15 +211,15 @@ def wall_from_params(x, params: dict, contour: str, xp=np):
     if contour == "conical":
         y_div = y_th + (y_ex - y_th) * s
     elif contour in ("bell", "smooth", "moc"):
-        y_div = _hermite(s, y_th, y_ex, xp.tan(xp.asarray(params["theta_initial"])) * dx_ds,
-                         xp.tan(xp.asarray(params["theta_exit"])) * dx_ds)
+        y_div = _hermite(s, y_th, y_ex, xp.tan(params["theta_initial"]) * dx_ds,
+                         xp.tan(params["theta_exit"]) * dx_ds)
     elif contour == "bezier":
         c1 = y_th + params["bezier_w1"] * (y_ex - y_th)
         c2 = y_th + params["bezier_w2"] * (y_ex - y_th)
         u = 1.0 - s
         y_div = u**3 * y_th + 3.0 * u**2 * s * c1 + 3.0 * u * s**2 * c2 + s**3 * y_ex
     else:
-        base = _hermite(s, y_th, y_ex, 0.0, xp.tan(xp.asarray(params["theta_exit"])) * dx_ds)
+        base = _hermite(s, y_th, y_ex, 0.0, xp.tan(params["theta_exit"]) * dx_ds)
         bump = sum(_bernstein(BEZIER8_DEGREE, k + 1, s) * params[f"offset_{k}"] for k in range(8))
         y_div = base + y_th * bump
     return xp.where(xi <= x_th, y_conv, y_div)
@@ -222,11 +228,11 @@ def wall_from_params(x, params: dict, contour: str, xp=np):
 def node_coords_from_params(x_frac, r_frac, params: dict, contour: str, xp=np):
     """Node coordinates ``(x, r y_wall(x))`` of the frozen logical grid (src/geometry/mesh.py:467-490)."""
     length = params.get("length", 1.0)
-    x = xp.asarray(x_frac) * length
+    x = _as_array(x_frac, xp) * length
     yw = wall_from_params(x, params, contour, xp)
     nr, nx = len(r_frac), len(x_frac)
     xx = xp.broadcast_to(x[None, :], (nr, nx))
-    yy = xp.asarray(r_frac)[:, None] * yw[None, :]
+    yy = _as_array(r_frac, xp)[:, None] * yw[None, :]
     return xp.stack([xx.reshape(-1), yy.reshape(-1)], -1)
 
 

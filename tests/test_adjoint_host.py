@@ -103,3 +103,27 @@ def test_differentiable_case_routes_keywords_and_freezes_the_grid():
     with pytest.raises(ValueError):
         dc.params_for(["nope"])
     assert set(ad.OBJECTIVES) == {"thrust", "thrust_coefficient", "exit_mach", "mass_flow", "exit_pressure"}
+
+
+@pytest.mark.parametrize("contour", ["smooth", "bell", "bezier8"])
+def test_node_coordinate_derivatives_match_central_differences(contour):
+    """torch's derivative of X(a) against central differences of the NumPy contour."""
+    import torch
+
+    ad, nz = pkg("adjoint"), pkg("nozzle")
+    kw = {"offsets": tuple(0.01 * np.cos(np.arange(8)))} if contour == "bezier8" else {}
+    dc = ad.differentiable_case(contour=contour, order=1, refine=0, device="cpu", **kw)
+    names = ["area_ratio", "throat_x", "throat_half_height", "inlet_half_height", "theta_exit", "length"]
+    names += ["offset_2"] if contour == "bezier8" else ["theta_initial"]
+    base = dc.default_params()
+    w = np.random.default_rng(0).standard_normal(dc.node_coords({}).shape)
+    for k in names:
+        P = {kk: torch.tensor(float(v), dtype=torch.float64, requires_grad=(kk == k)) for kk, v in base.items()}
+        X = dc.node_coords(P, xp=torch)
+        (g,) = torch.autograd.grad((X * torch.as_tensor(w)).sum(), [P[k]])
+        h = 1e-6 * max(1.0, abs(base[k]))
+        up, dn = dict(base), dict(base)
+        up[k] += h
+        dn[k] -= h
+        fd = np.sum(w * (dc.node_coords(up) - dc.node_coords(dn))) / (2 * h)
+        assert abs(float(g) - fd) <= 1e-6 * max(1.0, abs(fd)), (k, float(g), fd)
