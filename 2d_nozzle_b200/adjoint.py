@@ -489,7 +489,7 @@ class DifferentiableCase:
         R_a = {k: (float(gk) if gk is not None else 0.0) for k, gk in zip(P, rg)}
         grad = {k: J_a[k] - R_a[k] for k in base}
         self.last_adjoint = {"iterations": its, "relative_residual": rel, "lambda": lam}
-        return float(J), grad, fwd
+        return float(J.detach()), grad, fwd
 
 
 def differentiable_case(*, element="tri", order=1, refine=0, flow=None, options=None, device=None, **overrides):
