@@ -555,6 +555,182 @@ def check_gradient(case: DifferentiableCase, objective="thrust", params=None, *,
     return out
 
 
+
+
+# ---------------------------------------------------------------- many members at once
+class ObjectiveSpace:
+    """What :func:`objective_value` reads of one mesh: its operators, flow and element vertices."""
+
+    def __init__(self, ops, flow):
+        self.ops, self.flow = ops, flow
+        self.NV = 3 if ops.ref.kind == "tri" else 4
+        self.elem_nodes = np.ascontiguousarray(np.asarray(ops.topology.elem_nodes)[:, : self.NV])
+
+
+@dataclass
+class MemberGradient:
+    value: float
+    grad: dict | None
+    forward_status: str
+    forward_iterations: int
+    adjoint_converged: bool
+    adjoint_iterations: int
+    adjoint_residual: float
+
+
+class BatchGradient:
+    """Objective gradients of many design members of one case, marched together.
+
+    Per member this is :meth:`DifferentiableCase.value_and_gradient`
+    (src/sensitivity.py:386-460); all members' forward solves run as one
+    batched march (:class:`~.batch.BatchSolver`), all adjoint marches as one
+    ``nzb_adjoint`` object over the same concatenated mesh (each member retires
+    when its own defect meets the tolerance), and one ``nzb_vjp_coords`` launch
+    gives every member's ``lam^T dR/dX``.  The members share the case's
+    topology, order and solver options; they differ in design variables.
+    """
+
+    def __init__(self, case: DifferentiableCase, members, objective="thrust", names=None, device=None):
+        from .batch import Instance
+
+        self.case = case
+        self.members = [dict(m) for m in members]
+        if not self.members:
+            raise ValueError("no members")
+        self.objective = objective
+        self.names = tuple(names or self.members[0].keys())
+        self.device = torch.device(device if device is not None else (case.device or "cuda"))
+        self.cases = [case.case_at(m) for m in self.members]
+        self.instances = [Instance(cs.operators, cs.flow, case.options, cs.initial_state(), float(cs.geometry.length))
+                          for cs in self.cases]
+
+    def _params(self, i):
+        merged = self.case._merged(self.members[i])
+        P = {k: torch.tensor(float(merged[k]), dtype=torch.float64, device=self.device, requires_grad=True)
+             for k in self.names}
+        full = {k: P[k] if k in P else torch.tensor(float(v), dtype=torch.float64, device=self.device)
+                for k, v in merged.items()}
+        return P, full
+
+    def run(self, *, adjoint_tolerance=1e-8, max_iterations=100_000, check_interval=100) -> list[MemberGradient]:
+        from .batch import BatchSolver
+
+        lib = capi.load()
+        dev = self.device
+        fwd = BatchSolver(self.instances, device=dev)
+        fwd.run()
+        fres = fwd.results(with_state=False)
+        if len(fwd.meshes) != 1:
+            raise NotImplementedError("the members of one batch share the element kind and order")
+        dm = fwd.meshes[0]
+        S0 = fwd.buffers[0][1][0]
+        E, NP, NV, n = dm.E, dm.np_, dm.nf, len(self.members)
+        stream = dm.stream()
+
+        # seeds dJ/dU and the explicit dJ/da, member by member (boundary integrals in torch)
+        U_all = dm.unpack(S0)
+        seed = torch.zeros_like(U_all)
+        values = [float("nan")] * n
+        J_a = [None] * n
+        spans = [(int(fwd.local[i]), int(fwd.local[i]) + cs.operators.n_elem) for i, cs in enumerate(self.cases)]
+        for i, cs in enumerate(self.cases):
+            if not fres[i].converged:
+                continue
+            lo, hi = spans[i]
+            P, full = self._params(i)
+            Ui = U_all[lo:hi].clone().requires_grad_(True)
+            X = self.case.node_coords(full, xp=torch)
+            J = objective_value(ObjectiveSpace(cs.operators, cs.flow), Ui, X, self.objective, full)
+            g = torch.autograd.grad(J, [Ui] + list(P.values()), allow_unused=True)
+            seed[lo:hi] = g[0]
+            values[i] = float(J.detach())
+            J_a[i] = {k: float(gk) if gk is not None else 0.0 for k, gk in zip(P, g[1:])}
+
+        # every member's adjoint march in one object; failed forward solves never start
+        status = torch.tensor([0 if r.converged else 6 for r in fres], dtype=torch.int32, device=dev)
+        mesh = capi.Mesh()
+        C.memmove(C.byref(mesh), C.byref(dm.c), C.sizeof(capi.Mesh))
+        mesh.inst_status = status.data_ptr()
+        ph = fwd.phys[0]
+        size = 4 * NP * E
+        U_soa = S0
+        seed_soa = to_soa(seed)
+        z = lambda: torch.zeros(size, dtype=torch.float64, device=dev)  # noqa: E731
+        lam, Y1, Y2, f0, f1, f2, scratch = (z() for _ in range(7))
+        wave = torch.zeros(E, dtype=torch.float64, device=dev)
+        dt = torch.zeros(E, dtype=torch.float64, device=dev)
+        capi.check(lib.nzb_residual(C.byref(mesh), C.byref(ph), 0, U_soa.data_ptr(), scratch.data_ptr(),
+                                    wave.data_ptr(), stream), "nzb_residual")
+        coef = step_coefficient(self.cases[0].operators.ref.order, self.case.options.cfl, "ssprk3")
+        capi.check(lib.nzb_local_dt(C.byref(mesh), wave.data_ptr(), coef, dt.data_ptr(), stream), "nzb_local_dt")
+        bf = capi.AdjointBuffers()
+        bf.U, bf.seed, bf.lam, bf.Y1, bf.Y2 = (t.data_ptr() for t in (U_soa, seed_soa, lam, Y1, Y2))
+        bf.f0, bf.f1, bf.f2, bf.dt = (t.data_ptr() for t in (f0, f1, f2, dt))
+        t = {"elem_norm": torch.zeros(E, dtype=torch.float64, device=dev),
+             "iterations": torch.zeros(n, dtype=torch.int32, device=dev),
+             "res0": torch.zeros(n, dtype=torch.float64, device=dev),
+             "res": torch.zeros(n, dtype=torch.float64, device=dev),
+             "n_running": torch.zeros(1, dtype=torch.int32, device=dev)}
+        am = capi.AdjointMarch()
+        am.n_inst = n
+        am.inst_begin, am.inst_end, am.inst_count = (fwd.t[k].data_ptr() for k in ("begin", "end", "count"))
+        am.elem_norm, am.status = t["elem_norm"].data_ptr(), status.data_ptr()
+        am.iterations, am.res0, am.res = (t[k].data_ptr() for k in ("iterations", "res0", "res"))
+        am.n_running = t["n_running"].data_ptr()
+        am.tolerance = float(adjoint_tolerance)
+        am.max_iterations = int(max_iterations)
+        offs = np.zeros(1, np.int64)
+        h = capi.P()
+        capi.check(lib.nzb_adjoint_create(1, C.byref(mesh), C.byref(ph), C.byref(bf), offs.ctypes.data, C.byref(am),
+                                          C.byref(h)), "nzb_adjoint_create")
+        try:
+            capi.check(lib.nzb_adjoint_run(h.value, 0, stream), "nzb_adjoint_run")
+            done = 0
+            while int(t["n_running"].item()) > 0 and done < max_iterations:
+                k = min(check_interval, max_iterations - done)
+                capi.check(lib.nzb_adjoint_run(h.value, k, stream), "nzb_adjoint_run")
+                done += k
+        finally:
+            lib.nzb_adjoint_destroy(h.value)
+        ast = status.cpu().numpy()
+        its = t["iterations"].cpu().numpy()
+        rel = (t["res"] / torch.where(t["res0"] > 0, t["res0"], torch.ones_like(t["res0"]))).cpu().numpy()
+
+        # lam^T dR/dX of every member whose adjoint converged, in one launch
+        include = torch.where(status == 1, 0, 7).to(torch.int32)
+        mesh.inst_status = include.data_ptr()
+        verts_h = np.concatenate([np.asarray(cs.operators.node_coords)[ObjectiveSpace(cs.operators, cs.flow).elem_nodes]
+                                  for cs in self.cases])  # (E, NV, 2)
+        verts = torch.as_tensor(np.ascontiguousarray(np.concatenate([verts_h[:, :, 0].T, verts_h[:, :, 1].T])),
+                                device=dev)
+        gvert = torch.zeros(2 * NV * E, dtype=torch.float64, device=dev)
+        gpb = torch.zeros(E, dtype=torch.float64, device=dev)
+        dgs = np.ascontiguousarray(face_tangent_table(self.cases[0].operators.ref).ravel())
+        capi.check(lib.nzb_vjp_coords(C.byref(mesh), C.byref(ph), U_soa.data_ptr(), lam.data_ptr(), verts.data_ptr(),
+                                      dgs.ctypes.data, gvert.data_ptr(), gpb.data_ptr(), stream), "nzb_vjp_coords")
+        gv = gvert.reshape(2, NV, E).cpu().numpy()
+        gp = gpb.cpu().numpy()
+
+        out = []
+        for i, cs in enumerate(self.cases):
+            grad = None
+            if ast[i] == 1:
+                lo, hi = spans[i]
+                en = ObjectiveSpace(cs.operators, cs.flow).elem_nodes
+                g = np.zeros((np.asarray(cs.operators.node_coords).shape[0], 2))
+                np.add.at(g[:, 0], en.T, gv[0][:, lo:hi])
+                np.add.at(g[:, 1], en.T, gv[1][:, lo:hi])
+                P, full = self._params(i)
+                X = self.case.node_coords(full, xp=torch)
+                L = (torch.as_tensor(g, device=dev) * X).sum() + float(np.sum(gp[lo:hi])) * full["back_pressure"]
+                rg = torch.autograd.grad(L, list(P.values()), allow_unused=True)
+                grad = {k: J_a[i][k] - (float(gk) if gk is not None else 0.0) for k, gk in zip(P, rg)}
+            out.append(MemberGradient(values[i], grad, fres[i].status, fres[i].iterations, bool(ast[i] == 1),
+                                      int(its[i]), float(rel[i])))
+        return out
+
+
 __all__ = ["OBJECTIVES", "FLOW_DESIGN_PARAMETERS", "AdjointModel", "AdjointMarch", "ResidualFunction",
            "DifferentiableCase", "differentiable_case", "objective_value", "finite_difference_gradient",
-           "check_gradient", "face_tangent_table", "to_soa", "from_soa"]
+           "check_gradient", "face_tangent_table", "to_soa", "from_soa", "BatchGradient", "MemberGradient",
+           "ObjectiveSpace"]

@@ -48,18 +48,20 @@ def units() -> list[str]:
     return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, defines=(), out: str | None = None) -> str:
+    """Build the library (``out``: another path, ``defines``: extra -D macros, e.g. launch bounds)."""
+    lib = out or LIB
+    if not force and not defines and out is None and up_to_date():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     tag = f"tmp{os.getpid()}"
     flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
-             "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+             "-I", os.path.join(ROOT, "include"), "-I", CSRC, *[f"-D{d}" for d in defines]]
     if verbose:
         flags.insert(0, "-Xptxas=-v")
     objs, procs = [], []
     for src in units():
-        obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + f".{tag}.o")
+        obj = os.path.join(os.path.dirname(lib), os.path.basename(src)[:-3] + f".{tag}.o")
         objs.append(obj)
         procs.append((src, subprocess.Popen([nvcc(), *flags, "-c", src, "-o", obj], stdout=subprocess.PIPE,
                                             stderr=subprocess.PIPE, text=True)))
@@ -73,17 +75,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     try:
         if errors:
             raise RuntimeError("\n".join(errors))
-        tmp = LIB + f".{tag}"
+        tmp = lib + f".{tag}"
         res = subprocess.run([nvcc(), *ARCH, "-shared", "-cudart", "static", *objs, "-o", tmp], capture_output=True,
                              text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed ({res.returncode}):\n{res.stderr[-6000:]}")
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib)
     finally:
         for o in objs:
             if os.path.exists(o):
                 os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

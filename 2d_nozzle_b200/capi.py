@@ -11,7 +11,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libnozzle_b200.so")
+# NZB_LIBRARY names another build of the same library (e.g. one compiled with
+# different launch bounds); by default the in-tree build is loaded.
+LIB_PATH = os.environ.get("NZB_LIBRARY") or os.path.join(_HERE, "_lib", "libnozzle_b200.so")
 
 P = C.c_void_p
 I64 = C.c_int64

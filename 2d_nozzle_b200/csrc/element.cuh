@@ -313,10 +313,22 @@ __device__ __forceinline__ void block_sum_store(double v, double* dst) {
 
 // Threads per block: 128, or 64 where the per-thread face accumulator would
 // push static shared memory past 48 KB (cubic quadrilaterals).
+//
+// MINB_* is the minimum of resident blocks per SM asked of the compiler
+// (__launch_bounds__), which caps registers per thread at 65536 / (MINB * NT).
+#ifndef NZB_MINB_RES
+#define NZB_MINB_RES 1
+#endif
+#ifndef NZB_MINB_STAGE
+#define NZB_MINB_STAGE 1
+#endif
 template <int K, int P>
 struct Launch {
   static constexpr int NP = Shape<K, P>::NP;
   static constexpr int NT = (NP * 4 * 8 * 128 <= 40 * 1024) ? 128 : 64;
+  // counted in 128-thread blocks: a 64-thread block asks for twice as many
+  static constexpr int MINB_RES = NZB_MINB_RES * 128 / NT;
+  static constexpr int MINB_STAGE = NZB_MINB_STAGE * 128 / NT;
 };
 
 // Face bits of this element (bit f = its side of face f) from the mesh arrays.
@@ -332,7 +344,8 @@ __device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
 // and the limiter (a smaller kernel: fewer registers, no instruction-cache
 // pressure from code it never runs); LIM = true handles stages and the limiter.
 template <int K, int P, bool AFF, bool LIM>
-__global__ void __launch_bounds__(Launch<K, P>::NT) k_element(const nzb_mesh m, const nzb_physics ph, const Work w) {
+__global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STAGE : Launch<K, P>::MINB_RES)
+    k_element(const nzb_mesh m, const nzb_physics ph, const Work w) {
   using S = Shape<K, P>;
   constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
   constexpr int BT = Launch<K, P>::NT;

@@ -136,3 +136,37 @@ def test_published_gradients(cuda):
                  "inlet_half_height": -1.524949e+00, "back_pressure": 0.0, "length": 1.353855e-2}
     for k, v in published.items():
         assert abs(grad[k] - v) <= 1e-6 * abs(v) + 1e-12, (k, grad[k], v)
+
+
+def bezier8_members(n, sigma=0.02, seed=0):
+    """Eight radial wall offsets per member, Gaussian with sigma (a fraction of the throat half-height)."""
+    rng = np.random.default_rng(seed)
+    return [{f"offset_{k}": float(v) for k, v in enumerate(rng.normal(0.0, sigma, 8))} for _ in range(n)]
+
+
+def test_batched_gradients_match_one_at_a_time(cuda):
+    ad = pkg("adjoint")
+    dc = ad.differentiable_case(contour="smooth", order=1, refine=0, back_pressure_ratio=0.15, tolerance=1e-11)
+    members = [{"area_ratio": a, "throat_x": 0.1388} for a in (2.3, 2.5, 2.7)]
+    out = ad.BatchGradient(dc, members, "thrust").run()
+    for m, r in zip(members, out):
+        assert r.forward_status == "converged" and r.adjoint_converged
+        value, grad, fwd = dc.value_and_gradient("thrust", m, names=tuple(m))
+        assert fwd.iterations == r.forward_iterations
+        assert abs(r.value - value) <= 1e-12 * abs(value)
+        for k in m:
+            assert abs(r.grad[k] - grad[k]) <= 1e-7 * max(abs(grad[k]), 1e-8), (k, r.grad[k], grad[k])
+
+
+def test_bezier8_shape_gradient_matches_central_differences(cuda):
+    """Eight-offset wall, AR 2.5, p = 2 triangles, refine 2, AUSM+-up: adjoint vs central differences."""
+    ad = pkg("adjoint")
+    m0 = bezier8_members(1, seed=4)[0]
+    dc = ad.differentiable_case(contour="bezier8", area_ratio=2.5, order=2, refine=2, flux="ausmup",
+                                back_pressure_ratio=0.15, tolerance=1e-11, offsets=tuple(m0.values()))
+    names = ("offset_1", "offset_5")
+    value, grad, fwd = dc.value_and_gradient("thrust", names=names, adjoint_tolerance=1e-10)
+    assert fwd.converged
+    fd = ad.finite_difference_gradient(dc, "thrust", names=names, step=1e-6)
+    for k in names:
+        assert abs(grad[k] - fd[k]) <= 1e-4 * abs(fd[k]) + 1e-9, (k, grad[k], fd[k])
