@@ -478,28 +478,45 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
     }
     if (w.wave) w.wave[e] = wave;
 
-    // ---- volume term, fully unrolled, tables as constant-bank operands
+    // ---- volume term, fully unrolled, tables as constant-bank operands.
+    // With NP >= 9 the coefficients and the accumulators together would not fit
+    // in registers, so the coefficients move into this thread's shared-memory
+    // column (free once its face sums are in the accumulators).
+    constexpr bool USM = NP >= 9;
     double acc[NP][4];
     {
-      double u[NP][4];
+      double u[USM ? 1 : NP][4];
 #pragma unroll
       for (int i = 0; i < NP; ++i)
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-          u[i][s] = __ldg(w.V + (s * NP + i) * E + e);
           acc[i][s] = facc[(i * 4 + s) * BT + t];
+          const double v = __ldg(w.V + (s * NP + i) * E + e);
+          if constexpr (USM)
+            facc[(i * 4 + s) * BT + t] = v;
+          else
+            u[i][s] = v;
         }
+      auto coef = [&](int i, int s) -> double {
+        if constexpr (USM)
+          return facc[(i * 4 + s) * BT + t];
+        else
+          return u[i][s];
+      };
       // affine: (xi_x F + xi_y G) det, det only for the residual (the rate
       // divides it out again); general: det (xi_x, xi_y) = (y_eta, -x_eta)
       const double vs = AFF ? (rate ? 1.0 : -det) : -1.0;
-#pragma unroll
+      // cubic quadrilaterals: a rolled point loop (64 accumulators leave no
+      // room for a fully unrolled one)
+      constexpr int QUNROLL = NP >= 16 ? 1 : NQV;
+#pragma unroll QUNROLL
       for (int q = 0; q < NQV; ++q) {
         double uq[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < NP; ++i) {
           const double phi = tab<K, P>(S::O_PHI + i * NQV + q);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) uq[s] = fma(phi, u[i][s], uq[s]);
+          for (int s = 0; s < 4; ++s) uq[s] = fma(phi, coef(i, s), uq[s]);
         }
         const Prim pr = primitives_fast(uq, g);
         const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
@@ -545,44 +562,64 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
           dt = w.dt[e];
         }
       }
-      // rate = -M^-1 R, one component at a time so its accumulators retire as
-      // the new state is formed
-      double u[NP][4];
+      // rate = -M^-1 R row by row: each inverse-mass entry is loaded once and
+      // used at once; the new state goes to this thread's shared-memory column
+      // in place of the old one (USM) or to registers
+      const bool stage = LIM && w.op == OP_STAGE;
+      double u[USM ? 1 : NP][4];
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
+      for (int i = 0; i < NP; ++i) {
+        double r[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-        for (int i = 0; i < NP; ++i) {
-          double r = 0.0;
-          if (AFF) {
+        for (int j = 0; j < NP; ++j) {
+          const double mij = AFF ? tab<K, P>(S::O_MINV + i * NP + j) : __ldg(m.minv + (i * NP + j) * E + e);
 #pragma unroll
-            for (int j = 0; j < NP; ++j) r = fma(tab<K, P>(S::O_MINV + i * NP + j), acc[j][s], r);
-          } else {
+          for (int s = 0; s < 4; ++s) r[s] = fma(mij, acc[j][s], r[s]);
+        }
 #pragma unroll
-            for (int j = 0; j < NP; ++j) r = fma(__ldg(m.minv + (i * NP + j) * E + e), acc[j][s], r);
-            r = -r;
+        for (int s = 0; s < 4; ++s) {
+          if (!AFF) r[s] = -r[s];
+          if (!stage) {
+            w.out[(s * NP + i) * E + e] = r[s];
+            continue;
           }
-          if (!LIM || w.op == OP_RATE) {
-            w.out[(s * NP + i) * E + e] = r;
+          double v;
+          if constexpr (USM)
+            v = facc[(i * 4 + s) * BT + t];
+          else
+            v = __ldg(w.V + (s * NP + i) * E + e);
+          double un;
+          if (w.stage == 1) {
+            const double rw = r[s] * ph.norm_w[s];
+            nrm = fma(rw, rw, nrm);
+            un = v + dt * r[s];
           } else {
-            const double v = __ldg(w.V + (s * NP + i) * E + e);
-            if (w.stage == 1) {
-              const double rw = r * ph.norm_w[s];
-              nrm = fma(rw, rw, nrm);
-              u[i][s] = v + dt * r;
-            } else {
-              const double u0 = __ldg(w.U0 + (s * NP + i) * E + e);
-              u[i][s] = w.a * u0 + w.b * (v + dt * r);
-            }
+            const double u0 = __ldg(w.U0 + (s * NP + i) * E + e);
+            un = w.a * u0 + w.b * (v + dt * r[s]);
           }
+          if constexpr (USM)
+            facc[(i * 4 + s) * BT + t] = un;
+          else
+            u[i][s] = un;
         }
       }
-      if (LIM && w.op == OP_STAGE) {
+      if (stage) {
         if (w.elem_norm && w.stage == 1) w.elem_norm[e] = nrm;
-        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, sides, scaled, repaired);
+        double ul[NP][4];
 #pragma unroll
         for (int i = 0; i < NP; ++i)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = u[i][s];
+          for (int s = 0; s < 4; ++s) {
+            if constexpr (USM)
+              ul[i][s] = facc[(i * 4 + s) * BT + t];
+            else
+              ul[i][s] = u[i][s];
+          }
+        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(ul, m, ph, e, sides, scaled, repaired);
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = ul[i][s];
         if (w.flags) w.flags[e] = (uint8_t)(scaled | (repaired << 1));
       }
     }
