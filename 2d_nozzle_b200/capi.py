@@ -25,7 +25,7 @@ class Mesh(C.Structure):
         ("kind", I32),
         ("order", I32),
         ("affine", I32),
-        ("reserved", I32),
+        ("edge_pass", I32),
         ("n_elem", I64),
         ("n_edge", I64),
         ("geo", P),
@@ -38,6 +38,9 @@ class Mesh(C.Structure):
         ("elem_inst", P),
         ("inst_status", P),
         ("inst_p_back", P),
+        ("edge_conn", P),
+        ("edge_flux", P),
+        ("edge_speed", P),
     ]
 
 

@@ -7,7 +7,9 @@
 
 #include "adjoint.cuh"
 
+#ifndef NZB_INTERNAL
 #define NZB_INTERNAL __attribute__((visibility("hidden")))
+#endif
 
 namespace nzb {
 

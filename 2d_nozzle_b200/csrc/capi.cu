@@ -16,6 +16,7 @@
 
 #include "adjoint_dispatch.cuh"
 #include "element.cuh"
+#include "forward_dispatch.cuh"
 #include "nozzle_b200.h"
 
 namespace nzb {
@@ -77,33 +78,14 @@ static int64_t element_blocks(const nzb_mesh& m) {
   return (m.n_elem + bt - 1) / bt;
 }
 
-template <int K, int P, bool AFF>
-static int launch_element(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
-  const int64_t nb = element_blocks(m);
-  if (nb > 0x7fffffff) return fail("too many elements for one launch");
-  if (w.op == OP_STAGE || w.op == OP_LIMIT)
-    k_element<K, P, AFF, true><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
-  else
-    k_element<K, P, AFF, false><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
-  return launch_check("element kernel launch");
-}
-
+// The element kernels live in forward_tri.cu / forward_quad.cu.
 static int dispatch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
-#define NZB_CASE(K, P)                                                                \
-  if (m.kind == K && m.order == P) {                                                  \
-    if (K == 0 && m.affine) return launch_element<K, P, (K == 0)>(m, ph, w, st);      \
-    return launch_element<K, P, false>(m, ph, w, st);                                 \
-  }
-  NZB_CASE(0, 0)
-  NZB_CASE(0, 1)
-  NZB_CASE(0, 2)
-  NZB_CASE(0, 3)
-  NZB_CASE(1, 0)
-  NZB_CASE(1, 1)
-  NZB_CASE(1, 2)
-  NZB_CASE(1, 3)
-#undef NZB_CASE
-  return fail("unsupported kind/order");
+  if (element_blocks(m) > 0x7fffffff || (m.edge_pass && (m.n_edge + 127) / 128 > 0x7fffffff))
+    return fail("too many elements for one launch");
+  if (m.edge_pass && w.op != OP_LIMIT && (!m.edge_conn || !m.edge_flux || !m.edge_speed))
+    return fail("the edge pass needs edge_conn, edge_flux and edge_speed");
+  const cudaError_t e = m.kind == NZB_TRI ? element_launch_tri(m, ph, w, st) : element_launch_quad(m, ph, w, st);
+  return cuda_check(e, "element kernel launch");
 }
 
 // ---- layout conversion ------------------------------------------------------
@@ -649,6 +631,8 @@ int nzb_upload_tables(int kind, int order, const double* tables, int64_t n) {
   // every translation unit holds its own copy of the tables
   const size_t off = (size_t)slot_offset(kind, order);
   if (cuda_check(cudaMemcpyToSymbol(c_tab, tables, sizeof(double) * n, sizeof(double) * off), "table upload") ||
+      cuda_check(upload_tables_fwd_tri(tables, (size_t)n, off), "table upload (triangles)") ||
+      cuda_check(upload_tables_fwd_quad(tables, (size_t)n, off), "table upload (quadrilaterals)") ||
       cuda_check(upload_tables_tri(tables, (size_t)n, off), "table upload (adjoint, triangles)") ||
       cuda_check(upload_tables_quad(tables, (size_t)n, off), "table upload (adjoint, quadrilaterals)"))
     return -1;

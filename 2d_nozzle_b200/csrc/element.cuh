@@ -340,10 +340,81 @@ __device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
   return sides;
 }
 
+// The edge pass: one thread per edge evaluates the numerical flux at the
+// edge's points, once -- the owner's trace (phi_face[0, f]) as the left state,
+// the neighbour's (phi_face[1, nf]) as the right, the owner's normal -- and
+// stores w_q |dX/dsigma| Fhat (edge_flux, (NQF, 4, n_edge)) and max_q s_q
+// (edge_speed), the reference's edge_pass (src/backends/_numba_kernels.py:
+// 484-583).  The element kernel with EP = true lifts them.  The arithmetic is
+// the fused kernel's, so both variants give bit-identical residuals.
+template <int K, int P>
+__global__ void __launch_bounds__(128) k_edge(const nzb_mesh m, const nzb_physics ph, const double* __restrict__ V) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQF = S::NQF, NE = S::NE;
+  const int64_t NK = m.n_edge, E = m.n_elem;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= NK) return;
+  const int own = __ldg(m.edge_conn + k);
+  const int nb = __ldg(m.edge_conn + NK + k);
+  const int code = __ldg(m.edge_conn + 2 * NK + k);
+  const int f = code & 7, nf = (code >> 3) & 7, tag = code >> 6;
+  int inst = -1;
+  if (m.elem_inst) inst = __ldg(m.elem_inst + own);
+  if (inst >= 0 && __ldg(m.inst_status + inst) != 0) return;
+  const double p_back = (inst >= 0 && m.inst_p_back) ? __ldg(m.inst_p_back + inst) : ph.p_back;
+  const double nx = __ldg(m.edge_geo + 4 * k + 0);
+  const double ny = __ldg(m.edge_geo + 4 * k + 1);
+  const double jac = __ldg(m.edge_geo + 4 * k + 2);
+  double uo[NE][4], un[NE][4];
+#pragma unroll
+  for (int j = 0; j < NE; ++j) {
+    const int n = edge_node(K, P, f, j);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) uo[j][s] = __ldg(V + (s * NP + n) * E + own);
+  }
+  if (nb >= 0) {
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+      const int n = edge_node(K, P, nf, j);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) un[j][s] = __ldg(V + (s * NP + n) * E + nb);
+    }
+  }
+  double smax = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < NQF; ++q) {
+    double tc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < NE; ++j) {
+      const double c = pfe<K, P>(0, f, j, q);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) tc[s] = fma(c, uo[j][s], tc[s]);
+    }
+    double F[4], sp;
+    if (nb >= 0) {
+      double tn[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int j = 0; j < NE; ++j) {
+        const double c = pfe<K, P>(1, nf, j, q);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) tn[s] = fma(c, un[j][s], tn[s]);
+      }
+      sp = interface_flux(tc, tn, nx, ny, ph, F);
+    } else {
+      sp = boundary_flux(tag, tc, nx, ny, ph, p_back, F);
+    }
+    smax = sp > smax ? sp : smax;
+    const double scale = jac * c_tab[S::O_WF + q];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) m.edge_flux[(int64_t)(q * 4 + s) * NK + k] = F[s] * scale;
+  }
+  m.edge_speed[k] = smax;
+}
+
 // LIM = false compiles the residual / rate variant, without the stage update
 // and the limiter (a smaller kernel: fewer registers, no instruction-cache
 // pressure from code it never runs); LIM = true handles stages and the limiter.
-template <int K, int P, bool AFF, bool LIM>
+template <int K, int P, bool AFF, bool LIM, bool EP>
 __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STAGE : Launch<K, P>::MINB_RES)
     k_element(const nzb_mesh m, const nzb_physics ph, const Work w) {
   using S = Shape<K, P>;
@@ -401,6 +472,36 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
     const double fs = (AFF && rate) ? -1.0 / det : 1.0;
     double wave = 0.0;
     int sides = 0;
+    if constexpr (EP) {
+      // the edge pass (k_edge) has left w |dX/dsigma| Fhat at every edge point
+      // and max_q s_q per edge; lift them with this element's side of the face
+      const int64_t NK = m.n_edge;
+#pragma unroll 1
+      for (int f = 0; f < NF; ++f) {
+        const int code = __ldg(m.face_code + f * E + e);
+        const int k = __ldg(m.face_edge + f * E + e);
+        const int side = code & 1;
+        sides |= side << f;
+        const double coef = (side ? -1.0 : 1.0) * fs;
+#pragma unroll 1
+        for (int q = 0; q < NQF; ++q) {
+          double fwc[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) fwc[s] = __ldg(m.edge_flux + (int64_t)(q * 4 + s) * NK + k) * coef;
+#pragma unroll
+          for (int j = 0; j < NE; ++j) {
+            const double cj = pfe<K, P>(side, f, j, q);
+            const int n = edge_node(K, P, f, j);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+              double& a = facc[(n * 4 + s) * BT + t];
+              a = fma(cj, fwc[s], a);
+            }
+          }
+        }
+        wave += __ldg(m.edge_speed + k) * __ldg(m.edge_geo + 4 * (int64_t)k + 3);
+      }
+    } else {
 #pragma unroll 1
     for (int f = 0; f < NF; ++f) {
       const int code = __ldg(m.face_code + f * E + e);
@@ -475,6 +576,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
           }
       }
       wave += smax * len;
+    }
     }
     if (w.wave) w.wave[e] = wave;
 

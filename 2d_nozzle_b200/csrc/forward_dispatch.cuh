@@ -1,0 +1,21 @@
+// forward_dispatch.cuh -- launchers of the forward (residual / stage / limiter)
+// kernels, one translation unit per element kind (forward_tri.cu,
+// forward_quad.cu) so they compile in parallel.  Each unit holds its own copy
+// of the reference-element tables in constant memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "element.cuh"
+
+#ifndef NZB_INTERNAL
+#define NZB_INTERNAL __attribute__((visibility("hidden")))
+#endif
+
+namespace nzb {
+
+NZB_INTERNAL cudaError_t element_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st);
+NZB_INTERNAL cudaError_t element_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st);
+NZB_INTERNAL cudaError_t upload_tables_fwd_tri(const double* src, size_t count, size_t offset);
+NZB_INTERNAL cudaError_t upload_tables_fwd_quad(const double* src, size_t count, size_t offset);
+
+}  // namespace nzb

@@ -147,6 +147,13 @@ def host_arrays(ops, *, force_general: bool = False) -> dict:
     if np.abs(nrm - nrm[:, :1]).max() > 0.0 or np.abs(jac - jac[:, :1]).max() > 0.0:
         raise NotImplementedError("device kernels take straight edges (one normal per edge)")
     out["edge_geo"] = np.ascontiguousarray(np.stack([nrm[:, 0, 0], nrm[:, 0, 1], jac[:, 0], np.asarray(ops.edge_length)], axis=1))
+    # per edge: owner, neighbour (-1 on a boundary), owner face | neighbour face << 3 | tag << 6
+    ie, ifc = np.asarray(ed.iedge_elem), np.asarray(ed.iedge_face)
+    be, bfc, btag = np.asarray(ed.bedge_elem), np.asarray(ed.bedge_face), np.asarray(ed.bedge_tag)
+    owner = np.concatenate([ie[:, 0], be])
+    nbr_e = np.concatenate([ie[:, 1], np.full(be.shape, -1)])
+    code = np.concatenate([ifc[:, 0] | (ifc[:, 1] << 3), bfc | (btag << 6)])
+    out["edge_conn"] = np.ascontiguousarray(np.stack([owner, nbr_e, code]).astype(np.int32))
     return out
 
 
@@ -164,6 +171,9 @@ def concat_arrays(parts: list[dict]) -> dict:
     out["face_edge"] = np.ascontiguousarray(np.concatenate([p["face_edge"] + k_off[i] for i, p in enumerate(parts)], axis=1)
                                             .astype(np.int32))
     out["edge_geo"] = np.ascontiguousarray(np.concatenate([p["edge_geo"] for p in parts], axis=0))
+    out["edge_conn"] = np.ascontiguousarray(np.concatenate(
+        [np.stack([p["edge_conn"][0] + e_off[i], np.where(p["edge_conn"][1] >= 0, p["edge_conn"][1] + e_off[i], -1),
+                   p["edge_conn"][2]]) for i, p in enumerate(parts)], axis=1).astype(np.int32))
     if out["n_elem"] >= 2**31 or out["edge_geo"].shape[0] >= 2**31:
         raise ValueError("a bucket is limited to 2^31 elements and edges")
     return out
@@ -202,10 +212,26 @@ class DeviceMesh:
         m.affine = 1 if self.affine else 0
         m.n_elem = self.E
         m.n_edge = self.n_edge
-        for name in ("geo", "minv", "area", "face_nbr", "face_code", "face_edge", "edge_geo"):
+        for name in ("geo", "minv", "area", "face_nbr", "face_code", "face_edge", "edge_geo", "edge_conn"):
             setattr(m, name, keep[name].data_ptr() if name in keep else None)
+        # scratch of the edge pass: (NQF, 4, n_edge) fluxes and (n_edge) speeds
+        nqf = int(np.asarray(ref.w_face).shape[0])
+        self.edge_flux = torch.empty(nqf * 4 * self.n_edge, dtype=torch.float64, device=self.device)
+        self.edge_speed = torch.empty(self.n_edge, dtype=torch.float64, device=self.device)
+        m.edge_flux = self.edge_flux.data_ptr()
+        m.edge_speed = self.edge_speed.data_ptr()
+        m.edge_pass = 0
         self.c = m
         self.c_ref = C.byref(m)
+
+    @property
+    def edge_pass(self) -> bool:
+        return bool(self.c.edge_pass)
+
+    @edge_pass.setter
+    def edge_pass(self, on: bool) -> None:
+        """Face fluxes in a separate edge pass (True) or inside the element kernel (False)."""
+        self.c.edge_pass = 1 if on else 0
 
     def set_batch(self, elem_inst, inst_status, inst_p_back) -> None:
         """Attach the batch arrays (device tensors kept alive by the caller)."""

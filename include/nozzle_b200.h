@@ -67,12 +67,17 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * elem_inst   (E)      instance of each element (null: a single instance),
  * inst_status (n_inst) nonzero = retired: its elements are left untouched,
  * inst_p_back (n_inst) back pressure of each instance (null: phys.p_back).
+ * edge_pass = 1 splits every residual / stage into two launches: one thread
+ * per edge evaluates each edge's fluxes once (the reference's edge_pass), then
+ * the element kernel lifts them; edge_pass = 0 evaluates the fluxes inside the
+ * element kernel, from both sides.  Both give bit-identical results; which is
+ * faster depends on the element kind, order and mesh size.
  */
 typedef struct {
   int32_t kind;
   int32_t order;
   int32_t affine;
-  int32_t reserved;
+  int32_t edge_pass; /* 1: face fluxes in a separate edge pass (needs edge_conn, edge_flux, edge_speed) */
   int64_t n_elem;
   int64_t n_edge;
   const double* geo;
@@ -85,6 +90,10 @@ typedef struct {
   const int32_t* elem_inst;
   const int32_t* inst_status;
   const double* inst_p_back;
+  const int32_t* edge_conn; /* (3, n_edge): owner element, neighbour (-1: boundary),
+                               owner face | neighbour face << 3 | boundary tag << 6 */
+  double* edge_flux;        /* (NQF, 4, n_edge) scratch of the edge pass */
+  double* edge_speed;       /* (n_edge) scratch of the edge pass */
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly

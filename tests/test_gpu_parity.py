@@ -141,3 +141,23 @@ def test_norm_matches_the_oracle(cuda):
     ops, g = tiny_ops("tri", 3)
     bk = backend(ops)
     assert abs(bk.norm(g["U"]) - orc.norm(g["U"], bk.flow)) <= 1e-14 * orc.norm(g["U"], bk.flow)
+
+
+@pytest.mark.parametrize("kind,p", TINY)
+@pytest.mark.parametrize("flux", FLUXES)
+def test_edge_pass_is_bit_identical(cuda, kind, p, flux):
+    """The edge-pass variant and the fused variant give the same bits: residual, rate, wave and a stage."""
+    import torch
+
+    ops, g = tiny_ops(kind, p)
+    flow = pkg("config").FlowConditions(flux=flux, back_pressure_ratio=0.9)
+    bk = backend(ops, flow)
+    out = {}
+    for ep in (False, True):
+        bk.mesh.edge_pass = ep
+        R, wave = bk.residual(g["U"])
+        F, _ = bk.rate(g["U"])
+        U1, res, flags = bk.step_record(g["U"])
+        out[ep] = (R, wave, F, U1, res, flags)
+    for a, b in zip(out[False], out[True]):
+        assert np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
