@@ -615,11 +615,22 @@ class BatchGradient:
     def run(self, *, adjoint_tolerance=1e-8, max_iterations=100_000, check_interval=100) -> list[MemberGradient]:
         from .batch import BatchSolver
 
+        import time
+
         lib = capi.load()
         dev = self.device
+        clock = [time.perf_counter()]
+        self.timings = {}
+
+        def lap(name):
+            torch.cuda.synchronize(dev)
+            clock.append(time.perf_counter())
+            self.timings[name] = clock[-1] - clock[-2]
+
         fwd = BatchSolver(self.instances, device=dev)
         fwd.run()
         fres = fwd.results(with_state=False)
+        lap("forward")
         if len(fwd.meshes) != 1:
             raise NotImplementedError("the members of one batch share the element kind and order")
         dm = fwd.meshes[0]
@@ -646,6 +657,7 @@ class BatchGradient:
             values[i] = float(J.detach())
             J_a[i] = {k: float(gk) if gk is not None else 0.0 for k, gk in zip(P, g[1:])}
 
+        lap("seeds")
         # every member's adjoint march in one object; failed forward solves never start
         status = torch.tensor([0 if r.converged else 6 for r in fres], dtype=torch.int32, device=dev)
         mesh = capi.Mesh()
@@ -692,6 +704,7 @@ class BatchGradient:
                 done += k
         finally:
             lib.nzb_adjoint_destroy(h.value)
+        lap("adjoint")
         ast = status.cpu().numpy()
         its = t["iterations"].cpu().numpy()
         rel = (t["res"] / torch.where(t["res0"] > 0, t["res0"], torch.ones_like(t["res0"]))).cpu().numpy()
@@ -727,6 +740,7 @@ class BatchGradient:
                 grad = {k: J_a[i][k] - (float(gk) if gk is not None else 0.0) for k, gk in zip(P, rg)}
             out.append(MemberGradient(values[i], grad, fres[i].status, fres[i].iterations, bool(ast[i] == 1),
                                       int(its[i]), float(rel[i])))
+        lap("contraction")
         return out
 
 

@@ -18,6 +18,11 @@ status copied back.  ``plain`` marches a subset one instance at a time through
 the single-solve backend and the same subset as a batch: their ratio is the
 batched speed-up over the same attempted set.
 
+``adjoint`` times thrust gradients w.r.t. eight Bezier wall offsets for 64
+perturbed members (AR 2.5, p = 2 triangles, refine 2, AUSM+-up, forward and
+adjoint to 1e-10): all members as one batch (forward batch, one adjoint march
+object, one coordinate-VJP launch) against every 8th member one at a time.
+
 ``roofline`` is measured on the residual-kernel microbenchmark: 1,000,000
 straight-sided cubic triangles (Np = 10) on the unit rectangle, states drawn
 per node (density lognormal(0, 0.3), Mach U[0.2, 3] in a random direction,
@@ -275,6 +280,53 @@ def plain_solve(inst, torch):
     return bk, U0, scale
 
 
+def bezier8_members(n, sigma=0.02, seed=0):
+    """Eight radial wall offsets per member, Gaussian (sigma: a fraction of the throat half-height)."""
+    rng = np.random.default_rng(seed)
+    return [{f"offset_{k}": float(v) for k, v in enumerate(rng.normal(0.0, sigma, 8))} for _ in range(n)]
+
+
+def adjoint_section(args, torch):
+    """Batched vs one-at-a-time thrust gradients w.r.t. the 8 Bezier offsets (AR 2.5, p = 2 triangles,
+    refine 2, AUSM+-up, p_b 0.15; forward and adjoint to 1e-10)."""
+    ad = pkg("adjoint")
+    dc = ad.differentiable_case(contour="bezier8", area_ratio=2.5, order=2, refine=2, flux="ausmup",
+                                back_pressure_ratio=0.15, tolerance=1e-10, max_iterations=args.adjoint_cap)
+    members = bezier8_members(args.adjoint_members)
+    names = tuple(members[0])
+    bg = ad.BatchGradient(dc, members, "thrust", names=names)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = bg.run(adjoint_tolerance=1e-10)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    ok = [r for r in out if r.grad is not None]
+    sub = list(range(0, len(members), args.plain_stride))
+    t0 = time.perf_counter()
+    plain = {}
+    for i in sub:
+        try:
+            plain[i] = dc.value_and_gradient("thrust", members[i], names=names, adjoint_tolerance=1e-10)[1]
+        except RuntimeError:  # the member's forward or adjoint march failed, as in the batch
+            plain[i] = None
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    n_plain = sum(g is not None for g in plain.values())
+    diff = max([abs(out[i].grad[k] - g[k]) / max(abs(g[k]), 1e-12) for i, g in plain.items() for k in names
+                if g is not None and out[i].grad is not None] or [0.0])
+    return {"workload": f"{len(members)} bezier8 members (8 offsets, sigma 2% of the throat half-height, seed 0) "
+                        f"around AR 2.5, tri p=2 refine 2 (2240 elements), AUSM+-up, forward and adjoint to 1e-10",
+            "metric": "thrust gradients/s (8 design variables each)", "batched_gradients": len(ok),
+            "batched_seconds": t_batch, "batched_gradients_per_s": len(ok) / t_batch,
+            "plain_attempted": len(sub), "plain_gradients": n_plain, "plain_seconds": t_plain,
+            "plain_gradients_per_s": n_plain / t_plain, "speedup": (len(ok) / t_batch) / max(n_plain / t_plain, 1e-300),
+            "adjoint_iterations_max": max(r.adjoint_iterations for r in out),
+            "forward_iterations_max": max(r.forward_iterations for r in out),
+            "max_rel_diff_batched_vs_plain": diff, "batched_phases_s": bg.timings,
+            "forward_status": {st: sum(r.forward_status == st for r in out) for st in {r.forward_status for r in out}},
+            "forward_iteration_cap": args.adjoint_cap}
+
+
 def run_ours(args, rank, world, torch, dist):
     capi = pkg("capi")
     BatchSolver = pkg("batch").BatchSolver
@@ -401,6 +453,8 @@ def run_ours(args, rank, world, torch, dist):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if rank == 0 and args.adjoint_members > 0:
+        line["adjoint"] = adjoint_section(args, torch)
     if rank == 0 and not args.no_micro:
         mb = microbench(torch, capi, pkg("backend").B200Backend, pkg("config"), peak, peak_kind)
         line["roofline"] = mb.pop("roofline")
@@ -462,6 +516,8 @@ def main():
     ap.add_argument("--max-iterations", type=int, default=20000, help="iteration cap of every instance")
     ap.add_argument("--plain-stride", type=int, default=8, help="plain-vs-batched subset: every n-th built point")
     ap.add_argument("--no-micro", action="store_true")
+    ap.add_argument("--adjoint-members", type=int, default=64, help="batched-gradient members (0: skip)")
+    ap.add_argument("--adjoint-cap", type=int, default=100000, help="forward iteration cap of the gradient members")
     ap.add_argument("--cpu-seconds", type=float, default=18.0)
     ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
     ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
