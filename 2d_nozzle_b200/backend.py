@@ -26,7 +26,7 @@ import numpy as np
 
 from . import capi
 from .config import FLOOR, SCHEMES, recommended_scheme, step_coefficient
-from .autotune import tune_edge_pass
+from .autotune import choose_variant
 from .layout import DeviceMesh, physics_struct
 
 
@@ -62,12 +62,8 @@ class B200Backend:
         self._res = torch.zeros(1, dtype=torch.float64, device=d)
         self._counters = torch.zeros(2, dtype=torch.int64, device=d)
         self._solvers: dict[str, int] = {}
-        # fused or edge-pass face fluxes: timed on a uniform subsonic state
-        S = self._S[0].view(4, self.mesh.np_, E)
-        g = flow.gamma
-        for s, v in enumerate((1.0, 0.3, 0.0, 1.0 / (g - 1.0) + 0.045)):
-            S[s].fill_(v)
-        tune_edge_pass(self.mesh, self.phys, self._S[0])
+        # fused or edge-pass face fluxes, fixed per element type
+        choose_variant(self.mesh)
 
     def __del__(self):
         lib = getattr(self, "lib", None)

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import capi
 from .config import FLUX_IDS, SCHEMES, recommended_scheme, residual_scale, step_coefficient
-from .autotune import tune_edge_pass
+from .autotune import choose_variant
 from .layout import DeviceMesh, concat_arrays, host_arrays, physics_struct
 
 STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "diverged", 4: "stalled", 5: "max_iterations"}
@@ -125,7 +125,7 @@ class BatchSolver:
             U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])
             dm.pack(U0, S[0])
             self.U0_soa.append(S[0].clone())
-            tune_edge_pass(dm, ph, S[0])
+            choose_variant(dm)
             self.h2d_bytes += U0.nbytes + sum(a.nbytes for a in arrays.values() if isinstance(a, np.ndarray))
             bf = capi.Buffers()
             bf.S0, bf.S1, bf.S2 = (x.data_ptr() for x in S)
