@@ -225,9 +225,14 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
         out["kernels"][name] = {"ms": t * 1e3, "alg_bytes_per_elem": b, "gbs": b * E / t / 1e9}
     dom = max(results, key=results.get)
     k = out["kernels"][dom]
+    # DRAM bytes per element of each kernel from an ncu capture of 490,000 cubic triangles
+    # (profiles/k_element_stage_tri_p3_490k.md), scaled to this launch by its element count
+    traffic = {"residual_roe": 1055.0, "stage1_hllc": 1135.0, "stage2_hllc": 1503.0, "stage3_hllc": 1447.0}
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": k["gbs"], "peak": peak_gbs, "unit": "GB/s",
-                       "frac": k["gbs"] / peak_gbs, "peak_source": peak_kind, "traffic": None,
-                       "workload": out["workload"]}
+                       "frac": k["gbs"] / peak_gbs, "peak_source": peak_kind,
+                       "traffic": traffic[dom] * E if dom in traffic else None,
+                       "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on 490,000 elements, "
+                                         "scaled by element count", "workload": out["workload"]}
     return out
 
 
