@@ -75,6 +75,36 @@ __device__ __forceinline__ Dual<N> cst(double x) {
   return Dual<N>(x);
 }
 
+// b = J_F(U)^T cF + J_G(U)^T cG for the Euler flux (F, G) of thermo.py:64-70,
+// from the closed-form Jacobians (u = m / rho, v = n / rho, q^2 = u^2 + v^2,
+// phi = (gamma - 1) q^2 / 2, H = (E + p) / rho):
+//   dF/dU = [0, 1, 0, 0; phi - u^2, (3 - gamma) u, -(gamma - 1) v, gamma - 1;
+//            -u v, v, u, 0; u (phi - H), H - (gamma - 1) u^2, -(gamma - 1) u v, gamma u]
+// and dG/dU likewise with the roles of u and v exchanged.  Returns false --
+// leaving b to the dual-number path -- where a floor of the density or the
+// pressure is active, whose derivative these formulas do not have.
+__device__ __forceinline__ bool euler_flux_vjp(const double (&U)[4], double g, const double (&cF)[4],
+                                               const double (&cG)[4], double (&b)[4]) {
+  const double rho = U[0];
+  if (!(rho >= FLOOR)) return false;
+  const double u = U[1] / rho, v = U[2] / rho;
+  const double q2 = u * u + v * v;
+  const double gm = g - 1.0;
+  const double p = gm * (U[3] - 0.5 * rho * q2);
+  if (!(p >= FLOOR)) return false;
+  const double H = (U[3] + p) / rho;
+  const double phi = 0.5 * gm * q2;
+  const double uv = u * v;
+  b[0] = cF[1] * (phi - u * u) - cF[2] * uv + cF[3] * u * (phi - H) - cG[1] * uv + cG[2] * (phi - v * v) +
+         cG[3] * v * (phi - H);
+  b[1] = cF[0] + cF[1] * (3.0 - g) * u + cF[2] * v + cF[3] * (H - gm * u * u) + cG[1] * v - cG[2] * gm * u -
+         cG[3] * gm * uv;
+  b[2] = -cF[1] * gm * v + cF[2] * u - cF[3] * gm * uv + cG[0] + cG[1] * u + cG[2] * (3.0 - g) * v +
+         cG[3] * (H - gm * v * v);
+  b[3] = gm * (cF[1] + cG[2]) + g * (cF[3] * u + cG[3] * v);
+  return true;
+}
+
 template <int K, int P, bool AFF>
 __global__ void __launch_bounds__(Launch<K, P>::NT) k_vjp(const nzb_mesh m, const nzb_physics ph, const AdjWork w) {
   using S = Shape<K, P>;
@@ -224,17 +254,20 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_vjp(const nzb_mesh m, cons
         cF[s] = vs * (a00 * lx[s] + a10 * le[s]);
         cG[s] = vs * (a01 * lx[s] + a11 * le[s]);
       }
-      D4 Uq[4], F[4], G[4];
-#pragma unroll
-      for (int s = 0; s < 4; ++s) Uq[s] = D4::seed(uq[s], s);
-      euler_flux(Uq, g, F, G);
       double b[4];
+      if (!euler_flux_vjp(uq, g, cF, cG, b)) {
+        // a floored density or pressure: differentiate the floored flux itself
+        D4 Uq[4], F[4], G[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        double acc = 0.0;
+        for (int s = 0; s < 4; ++s) Uq[s] = D4::seed(uq[s], s);
+        euler_flux(Uq, g, F, G);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) acc = fma(cF[s], F[s].d[u], fma(cG[s], G[s].d[u], acc));
-        b[u] = acc;
+        for (int u = 0; u < 4; ++u) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 0; s < 4; ++s) acc = fma(cF[s], F[s].d[u], fma(cG[s], G[s].d[u], acc));
+          b[u] = acc;
+        }
       }
 #pragma unroll
       for (int i = 0; i < NP; ++i) {

@@ -432,6 +432,34 @@ def run_ours(args, rank, world, torch, dist):
              "subset": f"every {args.plain_stride}th built point",
              "iterations_match": [r.iterations for r in b_res] == p_its}
 
+    # the whole sweep one solve at a time: a plain march's time is linear in its iterations, so each
+    # (kind, order, mesh) class's cost per iteration (500 iterations of one member, with the march's
+    # per-check read-back) times every instance's iteration count (the same in both paths)
+    key = lambda inst: (inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem)  # noqa: E731
+    first = {}
+    for inst in insts:
+        first.setdefault(key(inst), inst)
+    t_it = {}
+    for k, inst in first.items():
+        bk, U0, scale = plain_solve(inst, torch)
+        bk._S[0].copy_(U0)
+        bk.run_device(1)
+        bk.run_device(inst.opts.check_interval)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            bk.run_device(inst.opts.check_interval)
+            float(bk._res.item())
+        torch.cuda.synchronize()
+        t_it[k] = (time.perf_counter() - t0) / (10 * inst.opts.check_interval)
+        del bk
+    est_all = float(sum(r.iterations * t_it[key(inst)] for inst, r in zip(insts, res)))
+    est_sub = float(sum(it * t_it[key(inst)] for inst, it in zip(sub, p_its)))
+    plain.update({"all_instances_estimated_plain_seconds": est_all,
+                  "all_instances_batched_seconds": t_rank / args.steps,
+                  "speedup_all_instances": est_all / (t_rank / args.steps),
+                  "estimate_check": {"subset_estimated_seconds": est_sub, "subset_measured_seconds": float(np.sum(p_times))}})
+
     line = {
         "metric": "batched steady design-sweep solves/s at 1e-10 scaled residual (converged solves)",
         "value": value,
