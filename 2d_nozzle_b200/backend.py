@@ -38,8 +38,8 @@ class B200Backend:
 
         self.torch = torch
         self.ops, self.flow, self.opts = ops, flow, opts
-        if opts.limiter == "superbee":
-            raise NotImplementedError("the B200 backend implements limiter='positivity' and 'none'")
+        if opts.limiter not in ("positivity", "superbee", "none"):
+            raise ValueError(f"unknown limiter {opts.limiter!r}")
         self.scheme = recommended_scheme(ops.ref.order) if opts.scheme is None else opts.scheme
         if self.scheme not in SCHEMES:
             raise ValueError(f"unknown scheme {self.scheme!r}; choose from {SCHEMES}")

@@ -72,6 +72,9 @@ class BatchSolver:
                 raise ValueError("every instance of a batch must share the march options")
             if inst.flow.flux not in FLUX_IDS:
                 raise NotImplementedError(f"flux {inst.flow.flux!r}")
+            if o.limiter == "superbee":
+                raise NotImplementedError("the Superbee limiter's domain-wide scale is per solve: batch with "
+                                          "limiter='positivity' or 'none'")
         self.opts = opts0
         dev = torch.device(device if device is not None else "cuda")
         self.device = dev

@@ -41,6 +41,9 @@ class Mesh(C.Structure):
         ("edge_conn", P),
         ("edge_flux", P),
         ("edge_speed", P),
+        ("elem_share", P),
+        ("lim_means", P),
+        ("lim_scale", P),
     ]
 
 
@@ -67,6 +70,7 @@ class Physics(C.Structure):
         ("lim_steps", I32),
         ("reserved", I32),
         ("norm_w", C.c_double * 4),
+        ("tvb_constant", C.c_double),
     ]
 
 

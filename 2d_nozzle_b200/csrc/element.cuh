@@ -176,19 +176,13 @@ __device__ __forceinline__ double point_det(const double (&xv)[Shape<K, P>::NF],
   return x_xi * y_eta - x_eta * y_xi;
 }
 
-// Zhang-Shu positivity limiter of one element, in place
-// (src/spatial/limiter.py:103-243; the O(NP) Lebesgue screen of
-// src/backends/_numba_kernels.py:1010-1026 skips provably admissible elements).
+// Cell-average weights of element e: a table for affine elements (M = det
+// M_ref), else sum_q phi_iq w_q det_q / area, as the reference builds them
+// (src/spatial/operators.py:283-287).
 template <int K, int P, bool AFF>
-__device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], const nzb_mesh& m,
-                                              const nzb_physics& ph, int64_t e, int sides, int& scaled,
-                                              int& repaired) {
+__device__ __forceinline__ void mean_weights(const nzb_mesh& m, int64_t e, double (&mw)[Shape<K, P>::NP]) {
   using S = Shape<K, P>;
-  const double g = ph.gamma;
   const int64_t E = m.n_elem;
-  // cell-average weights: a table for affine elements (M = det M_ref), else
-  // sum_q phi_iq w_q det_q / area, as the reference builds them
-  double mw[S::NP];
   if (AFF) {
 #pragma unroll
     for (int i = 0; i < S::NP; ++i) mw[i] = tab<K, P>(S::O_MW + i);
@@ -212,6 +206,20 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
 #pragma unroll
     for (int i = 0; i < S::NP; ++i) mw[i] = mw[i] / area;
   }
+}
+
+// Zhang-Shu positivity limiter of one element, in place
+// (src/spatial/limiter.py:103-243; the O(NP) Lebesgue screen of
+// src/backends/_numba_kernels.py:1010-1026 skips provably admissible elements).
+template <int K, int P, bool AFF>
+__device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], const nzb_mesh& m,
+                                              const nzb_physics& ph, int64_t e, int sides, int& scaled,
+                                              int& repaired) {
+  using S = Shape<K, P>;
+  const double g = ph.gamma;
+  const int64_t E = m.n_elem;
+  double mw[S::NP];
+  mean_weights<K, P, AFF>(m, e, mw);
   double ub[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int i = 0; i < S::NP; ++i)

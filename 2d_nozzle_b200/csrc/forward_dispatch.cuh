@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "element.cuh"
+#include "slope.cuh"
 
 #ifndef NZB_INTERNAL
 #define NZB_INTERNAL __attribute__((visibility("hidden")))

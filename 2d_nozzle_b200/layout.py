@@ -88,7 +88,8 @@ def physics_struct(flow, opts, ref) -> capi.Physics:
     ph.entropy_fix = float(flow.entropy_fix)
     ph.hllc_low_mach = float(getattr(flow, "hllc_low_mach", 0.0))
     ph.flux = FLUX_IDS[flow.flux]
-    ph.limiter = 1 if (opts.limiter == "positivity" and ref.order > 0) else 0
+    ph.limiter = {"positivity": 1, "superbee": 2}.get(opts.limiter, 0) if ref.order > 0 else 0
+    ph.tvb_constant = float(getattr(opts, "tvb_constant", 50.0))
     at2 = g * float(flow.Rgas) * float(flow.total_temperature)
     ph.in_cos = float(np.cos(flow.inflow_angle))
     ph.in_sin = float(np.sin(flow.inflow_angle))
@@ -221,6 +222,15 @@ class DeviceMesh:
         m.edge_flux = self.edge_flux.data_ptr()
         m.edge_speed = self.edge_speed.data_ptr()
         m.edge_pass = 0
+        # Superbee limiter: each element's share of the domain's area and scratch
+        if "area" in arrays:
+            area = np.asarray(arrays["area"], float)
+            self.elem_share = torch.as_tensor(area / area.sum(), device=self.device)
+            m.elem_share = self.elem_share.data_ptr()
+        self.lim_means = torch.empty(4 * self.E, dtype=torch.float64, device=self.device)
+        self.lim_scale = torch.empty(4, dtype=torch.float64, device=self.device)
+        m.lim_means = self.lim_means.data_ptr()
+        m.lim_scale = self.lim_scale.data_ptr()
         self.c = m
         self.c_ref = C.byref(m)
 

@@ -67,6 +67,12 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * elem_inst   (E)      instance of each element (null: a single instance),
  * inst_status (n_inst) nonzero = retired: its elements are left untouched,
  * inst_p_back (n_inst) back pressure of each instance (null: phys.p_back).
+ * The Superbee slope limiter (physics limiter 2) needs the domain-wide maximum
+ * of the cell averages, so it applies to a mesh of one instance only (no
+ * elem_inst): stages and nzb_limit then run three passes after the element
+ * kernel -- cell averages, their maximum, the slope limiter with the
+ * positivity limiter -- and count an element as scaled when either limiter
+ * changed it.
  * edge_pass = 1 splits every residual / stage into two launches: one thread
  * per edge evaluates each edge's fluxes once (the reference's edge_pass), then
  * the element kernel lifts them; edge_pass = 0 evaluates the fluxes inside the
@@ -94,6 +100,9 @@ typedef struct {
                                owner face | neighbour face << 3 | boundary tag << 6 */
   double* edge_flux;        /* (NQF, 4, n_edge) scratch of the edge pass */
   double* edge_speed;       /* (n_edge) scratch of the edge pass */
+  const double* elem_share; /* (E) A_e / A_domain, for the Superbee limiter (limiter 2) */
+  double* lim_means;        /* (4, E) scratch of the Superbee limiter */
+  double* lim_scale;        /* (4) scratch of the Superbee limiter */
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly
@@ -103,7 +112,7 @@ typedef struct {
   double entropy_fix;
   double hllc_low_mach;
   int32_t flux;
-  int32_t limiter;        /* 0 none, 1 positivity (ignored at p = 0) */
+  int32_t limiter;        /* 0 none, 1 positivity, 2 Superbee TVB then positivity (ignored at p = 0) */
   /* inflow: cos/sin of the inflow angle, a_t^2 = gamma R T_t, a_t, rho_t */
   double in_cos, in_sin, in_at2, in_at, in_rho_t;
   /* outflow: back pressure, backflow reservoir density (0 = off), p_t, band */
@@ -114,6 +123,7 @@ typedef struct {
   int32_t reserved;
   /* residual-norm component weights (1, 1/a_t, 1/a_t, 1/a_t^2) */
   double norm_w[4];
+  double tvb_constant; /* Superbee's TVB constant (limiter 2) */
 } nzb_physics;
 
 /* Tables of one reference element: see the packer in layout.py for the order.

@@ -364,6 +364,51 @@ def positivity(U, ops, flow, fraction=1e-8, steps=12):
     return U, bad, repaired
 
 
+# ------------------------------------------------------------- slope limiter
+def superbee_pair(a, b):
+    """Roe's Superbee in its two-argument form, maxmod(minmod(2a, b), minmod(a, 2b))
+    (src/spatial/limiter.py:246-270)."""
+    def minmod(x, y):
+        return np.where(x * y <= 0.0, 0.0, np.where(_abs(x) < _abs(y), x, y))
+
+    def maxmod(x, y):
+        return np.where(x * y <= 0.0, 0.0, np.where(_abs(x) > _abs(y), x, y))
+
+    return maxmod(minmod(2.0 * a, b), minmod(a, 2.0 * b))
+
+
+def superbee(U, ops, tvb_constant=50.0, tol=1e-12):
+    """The Superbee TVB slope limiter (src/spatial/limiter.py:273-405): per element and face the own
+    increment d = (face-averaged own trace) - ubar against the jump a = ubar(neighbour) - ubar; a
+    face is quiet on a boundary, for |d| <= tol, or below the TVB threshold
+    tvb * (A_e / A_total) * max_e |ubar_s|; theta_e = min over faces and components of
+    clip(superbee(a, d) / d, 0, 1); U <- ubar + theta (U - ubar).  Returns (U_new, changed mask)."""
+    U = np.asarray(U, float)
+    if ops.ref.order == 0:
+        return U.copy(), np.zeros(U.shape[0], bool)
+    ubar = np.einsum("ei,eis->es", np.asarray(ops.mean_weights), U)
+    ed = ops.topology.edges
+    E = U.shape[0]
+    nface = ed.face_edge.shape[1]
+    nb = np.repeat(np.arange(E)[:, None], nface, axis=1)
+    nb[ed.iedge_elem[:, 0], ed.iedge_face[:, 0]] = ed.iedge_elem[:, 1]
+    nb[ed.iedge_elem[:, 1], ed.iedge_face[:, 1]] = ed.iedge_elem[:, 0]
+    interior = (nb != np.arange(E)[:, None])[..., None]
+    jump = ubar[nb] - ubar[:, None, :]
+    w = np.asarray(ops.ref.w_face)
+    dev = np.einsum("efiq,q,eis->efs", _face_tables(ops), w, U) / w.sum() - ubar[:, None, :]
+    allowed = superbee_pair(jump, dev)
+    safe = np.where(np.abs(dev) > tol, dev, 1.0)
+    theta_face = np.clip(allowed / safe, 0.0, 1.0)
+    area = np.asarray(ops.elem_area)
+    share = (area / area.sum())[:, None, None]
+    scale = np.abs(ubar).max(axis=0)[None, None, :]
+    quiet = (np.abs(dev) <= tol) | ~interior | (np.abs(dev) <= tvb_constant * share * scale)
+    theta = np.where(quiet, 1.0, theta_face).min(axis=(1, 2))
+    out = ubar[:, None, :] + theta[:, None, None] * (U - ubar[:, None, :])
+    return out, np.abs(out - U).max(axis=(1, 2)) > 0.0
+
+
 # ------------------------------------------------------------------ march
 def step_coefficient(order, cfl, scheme):
     table = {"ssprk3": (1.437, 2.337, 2.240), "euler": (1.169, 1.337, 0.775)}[scheme]
@@ -403,8 +448,10 @@ class Stepper:
         if self.opts.limiter == "none" or self.ops.ref.order == 0:
             self.stage_masks.append(np.zeros(U.shape[0], bool))
             return U
-        if self.opts.limiter != "positivity":
-            raise NotImplementedError("the oracle restates the positivity limiter only")
+        if self.opts.limiter == "superbee":
+            U, _ = superbee(U, self.ops, getattr(self.opts, "tvb_constant", 50.0))
+        elif self.opts.limiter != "positivity":
+            raise ValueError(f"unknown limiter {self.opts.limiter!r}")
         out, bad, _ = positivity(U, self.ops, self.flow)
         self.stage_masks.append(bad)
         return out

@@ -157,6 +157,31 @@ def small_cases():
             _save(f"tiny_{kind}_p{p}.npz", **arrays)
 
 
+def superbee_cases():
+    """The Superbee TVB slope limiter on a rough state of every tiny mesh, and three SSP-RK3 steps with it."""
+    from src.api import build_case
+    from src.backends import get_backend
+    from src.config import SolverOptions
+    from src.spatial import limiter as lim
+
+    for kind, orders in (("tri", (1, 2, 3)), ("quad", (1, 2, 3))):
+        for p in orders:
+            cs = build_case(contour="smooth", element=kind, order=p, refine=0)
+            ops = cs.operators
+            rng = np.random.default_rng(3)
+            base = np.array([2.0, 0.6, 0.02, 5.0])
+            U = np.ascontiguousarray(base * (1.0 + 0.15 * rng.standard_normal((ops.n_elem, ops.ref.n_basis, 4))))
+            arrays = {"U": U,
+                      "superbee": lim.superbee_limiter(U, ops, cs.flow, tvb_constant=50.0),
+                      "superbee_tvb0": lim.superbee_limiter(U, ops, cs.flow, tvb_constant=0.0),
+                      "superbee_positivity": lim.apply_limiter(U, ops, cs.flow, "superbee", tvb_constant=50.0)}
+            bk = get_backend("numpy", ops, cs.flow, SolverOptions(limiter="superbee", scheme="ssprk3"))
+            V, res = bk.run(U.copy(), 3, "ssprk3")
+            arrays["run3_ssprk3"] = np.asarray(V)
+            arrays["run3_ssprk3_res"] = np.float64(res)
+            _save(f"superbee_{kind}_p{p}.npz", **arrays)
+
+
 def rectangle_microbench():
     """Config-2 distribution at 20x10 cells, cubic triangles, unit rectangle."""
     from src.backends import get_backend
@@ -328,3 +353,5 @@ if __name__ == "__main__":
         batch_cases()
     if "sweep" in which:
         sweep_outcomes()
+    if "superbee" in which:
+        superbee_cases()

@@ -63,3 +63,20 @@ def test_microbench_distribution_step_and_limited_sets(flux):
     V, res = st.run(g["U"].copy(), 1)
     assert rel(V, g[f"step_{flux}"]) < 1e-12
     assert np.array_equal(np.stack(st.stage_masks), g[f"step_{flux}_limited"])
+
+
+@pytest.mark.parametrize("kind,p", [("tri", 1), ("tri", 2), ("tri", 3), ("quad", 1), ("quad", 2), ("quad", 3)])
+def test_oracle_superbee_matches_the_reference(kind, p):
+    """The Superbee TVB slope limiter, with and without the threshold, then positivity; and 3 SSP-RK3 steps."""
+    ops, _ = tiny_ops(kind, p)
+    g = golden(f"superbee_{kind}_p{p}.npz")
+    cfg = pkg("config")
+    flow = cfg.FlowConditions()
+    out, _ = orc.superbee(g["U"], ops, 50.0)
+    assert rel(out, g["superbee"]) < 1e-13
+    out0, changed0 = orc.superbee(g["U"], ops, 0.0)
+    assert rel(out0, g["superbee_tvb0"]) < 1e-13 and changed0.any()
+    assert rel(orc.positivity(out, ops, flow)[0], g["superbee_positivity"]) < 1e-13
+    st = orc.Stepper(ops, flow, cfg.SolverOptions(limiter="superbee", scheme="ssprk3"))
+    V, res = st.run(g["U"].copy(), 3)
+    assert rel(V, g["run3_ssprk3"]) < 1e-12 and abs(res - g["run3_ssprk3_res"]) <= 1e-12 * abs(g["run3_ssprk3_res"])
