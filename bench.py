@@ -415,12 +415,9 @@ def run_ours(args, rank, world, torch, dist):
         dist.barrier()
     n_conv = sum(r.converged for r in res)
     t_rank = float(np.sum(times))
-    t_max = t_rank
-    if dist is not None:
-        tt = torch.tensor([t_rank], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * n_conv * args.steps / t_max
+    replicas = pkg("replicas")
+    t_max = replicas.max_over_ranks(t_rank, dist, "cuda")
+    value = replicas.whole_job_rate(n_conv * args.steps, world, t_max)
     outcomes = {}
     for r in res:
         outcomes[r.status] = outcomes.get(r.status, 0) + 1
