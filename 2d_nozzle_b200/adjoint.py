@@ -601,7 +601,7 @@ class BatchGradient:
         self.names = tuple(names or self.members[0].keys())
         self.device = torch.device(device if device is not None else (case.device or "cuda"))
         self.cases = [case.case_at(m) for m in self.members]
-        self.instances = [Instance(cs.operators, cs.flow, case.options, cs.initial_state(), float(cs.geometry.length))
+        self.instances = [Instance(cs.operators, cs.flow, case.options, cs.initial_state(), float(cs.geometry.length), cs.geometry)
                           for cs in self.cases]
 
     def _params(self, i):

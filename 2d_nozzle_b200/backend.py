@@ -62,6 +62,7 @@ class B200Backend:
         self._res = torch.zeros(1, dtype=torch.float64, device=d)
         self._counters = torch.zeros(2, dtype=torch.int64, device=d)
         self._solvers: dict[str, int] = {}
+        self._obs = None
         # fused or edge-pass face fluxes, fixed per element type
         choose_variant(self.mesh)
 
@@ -161,6 +162,16 @@ class B200Backend:
         capi.check(self.lib.nzb_norm(src.data_ptr(), self.mesh.E, self.mesh.np_, w.ctypes.data, self._partial.data_ptr(),
                                      self._res.data_ptr(), self._stream), "nzb_norm")
         return float(self._host(self._res)[0])
+
+    def performance(self, U, geom=None) -> dict:
+        """The performance() metrics of a state (src/post/postprocess.py:193-255), integrated on the
+        device; ``geom`` adds the throat-normalised coefficients and the ideal thrust."""
+        from .observables import DeviceObservables
+
+        if self._obs is None:
+            self._obs = DeviceObservables(self.mesh, self.phys, [(self.ops, 0, 0)], [self.flow])
+        src = self.mesh.pack(U, self._S[0])
+        return self._obs.performance(src, [geom])[0]
 
     # -- integrators (host composition of the primitives, src/backends/base.py:155-190)
     def euler_step(self, U):

@@ -41,6 +41,7 @@ class Instance:
     opts: object
     U0: np.ndarray
     length: float = 1.0
+    geometry: object = None  # the nozzle geometry: adds the throat-normalised observables
 
 
 @dataclass
@@ -188,6 +189,7 @@ class BatchSolver:
         self.done = 0
         self.chunks = 0
         self.launches = 0
+        self._obs = None
 
     def __del__(self):
         if getattr(self, "handle", None):
@@ -241,3 +243,29 @@ class BatchSolver:
                     states[i] = full[self.local[i]:self.local[i] + self.instances[i].ops.n_elem]
         return [InstanceResult(STATUS[int(st[i])], int(st[i]) == 1, int(its[i]), float(res[i]), float(res0[i]),
                                states.get(i)) for i in range(len(self.instances))]
+
+    def observables(self) -> list[dict]:
+        """Every instance's performance() metrics (thrust in both forms, mass flows, exit averages,
+        entropy error), integrated on the device: one launch per bucket, and only the per-instance
+        sums leave the device."""
+        from .observables import DeviceObservables, from_sums
+
+        if self._obs is None:
+            self._obs = []
+            for dm, ph, mem in zip(self.meshes, self.phys, self.members):
+                parts, e_off, k_off = [], 0, 0
+                for i in mem:
+                    ops = self.instances[i].ops
+                    parts.append((ops, e_off, k_off))
+                    e_off += int(ops.n_elem)
+                    k_off += int(ops.n_interior + ops.n_boundary)
+                self._obs.append(DeviceObservables(dm, ph, parts, [self.instances[i].flow for i in mem]))
+        for ob, (bf, S) in zip(self._obs, self.buffers):
+            ob.launch(S[0])
+        out = [None] * len(self.instances)
+        for ob, mem in zip(self._obs, self.members):
+            sums = ob.out.cpu().numpy()
+            for j, i in enumerate(mem):
+                inst = self.instances[i]
+                out[i] = from_sums(sums[j], inst.flow, inst.geometry)
+        return out

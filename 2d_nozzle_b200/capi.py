@@ -178,6 +178,26 @@ class AdjointMarch(C.Structure):
 
 ADJ_VJP, ADJ_DEFECT, ADJ_RATE, ADJ_RK4 = 0, 1, 2, 3
 
+
+class ObsArgs(C.Structure):
+    _fields_ = [
+        ("U", P),
+        ("n_seg", I32),
+        ("reserved", I32),
+        ("bedges", P),
+        ("bseg", P),
+        ("eseg", P),
+        ("r_gas", C.c_double),
+        ("s_t", C.c_double),
+        ("out", P),
+    ]
+
+
+# column of each per-instance sum of nzb_observables
+(OBS_MOM_OUT, OBS_MOM_IN, OBS_WALL_PX, OBS_MASS_IN, OBS_MASS_OUT, OBS_EXIT_LEN, OBS_EXIT_MACH, OBS_EXIT_P,
+ OBS_EXIT_T, OBS_ENTROPY, OBS_AREA) = range(11)
+NOBS = 11
+
 # (name, restype, argtypes) of every exported symbol
 SIGNATURES = [
     ("nzb_version", C.c_int, []),
@@ -188,6 +208,7 @@ SIGNATURES = [
     ("nzb_unpack_state", C.c_int, [P, P, I64, C.c_int, P, P]),
     ("nzb_residual", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.c_int, P, P, P, P]),
     ("nzb_inverse_mass", C.c_int, [C.POINTER(Mesh), P, P, P]),
+    ("nzb_observables", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(ObsArgs), P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

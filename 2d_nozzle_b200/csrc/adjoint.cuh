@@ -69,12 +69,6 @@ struct CoordWork {
   double dgs[4][4];     // tangent of face f = sum_v dgs[f][v] X_v
 };
 
-// A dual number with a plain double's value and no derivative.
-template <int N>
-__device__ __forceinline__ Dual<N> cst(double x) {
-  return Dual<N>(x);
-}
-
 // b = J_F(U)^T cF + J_G(U)^T cG for the Euler flux (F, G) of thermo.py:64-70,
 // from the closed-form Jacobians (u = m / rho, v = n / rho, q^2 = u^2 + v^2,
 // phi = (gamma - 1) q^2 / 2, H = (E + p) / rho):
@@ -105,8 +99,15 @@ __device__ __forceinline__ bool euler_flux_vjp(const double (&U)[4], double g, c
   return true;
 }
 
+// Resident blocks per SM asked of the compiler for k_vjp (as NZB_MINB_* for
+// the forward kernels): registers per thread are capped at 65536 / (MINB * NT).
+#ifndef NZB_MINB_VJP
+#define NZB_MINB_VJP 1
+#endif
+
 template <int K, int P, bool AFF>
-__global__ void __launch_bounds__(Launch<K, P>::NT) k_vjp(const nzb_mesh m, const nzb_physics ph, const AdjWork w) {
+__global__ void __launch_bounds__(Launch<K, P>::NT, NZB_MINB_VJP * 128 / Launch<K, P>::NT)
+    k_vjp(const nzb_mesh m, const nzb_physics ph, const AdjWork w) {
   using S = Shape<K, P>;
   using D4 = Dual<4>;
   constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
@@ -184,20 +185,18 @@ __global__ void __launch_bounds__(Launch<K, P>::NT) k_vjp(const nzb_mesh m, cons
         double xi[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) xi[s] = nb >= 0 ? scale * (side ? ln[s] - lc[s] : lc[s] - ln[s]) : scale * lc[s];
+        // only the own trace is seeded; the neighbour's trace, the normal and
+        // the back pressure enter as plain numbers
         D4 own[4], F[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) own[s] = D4::seed(tc[s], s);
-        const D4 dnx = cst<4>(nx), dny = cst<4>(ny);
         if (nb >= 0) {
-          D4 other[4];
-#pragma unroll
-          for (int s = 0; s < 4; ++s) other[s] = cst<4>(tn[s]);
           if (side)
-            interface_flux(other, own, dnx, dny, ph, F);
+            interface_flux(tn, own, nx, ny, ph, F);
           else
-            interface_flux(own, other, dnx, dny, ph, F);
+            interface_flux(own, tn, nx, ny, ph, F);
         } else {
-          boundary_flux(tag, own, dnx, dny, ph, cst<4>(p_back), F);
+          boundary_flux(tag, own, nx, ny, ph, p_back, F);
         }
         double a[4];
 #pragma unroll
@@ -438,18 +437,13 @@ __global__ void __launch_bounds__(128) k_vjp_coords(const nzb_mesh m, const nzb_
         }
       }
       const double wq = c_tab[S::O_WF + q];
-      D3 UL[4], F[4];
-#pragma unroll
-      for (int s = 0; s < 4; ++s) UL[s] = cst<3>(tc[s]);
+      // seeded on (n_x, n_y, p_back); the traces enter as plain numbers
+      D3 F[4];
       const D3 dnx = D3::seed(nx, 0), dny = D3::seed(ny, 1);
-      if (nb >= 0) {
-        D3 UR[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) UR[s] = cst<3>(tn[s]);
-        interface_flux(UL, UR, dnx, dny, ph, F);
-      } else {
-        boundary_flux(tag, UL, dnx, dny, ph, D3::seed(p_back, 2), F);
-      }
+      if (nb >= 0)
+        interface_flux(tc, tn, dnx, dny, ph, F);
+      else
+        boundary_flux(tag, tc, dnx, dny, ph, D3::seed(p_back, 2), F);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const double xs = wq * (nb >= 0 ? lc[s] - ln[s] : lc[s]);

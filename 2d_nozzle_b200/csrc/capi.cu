@@ -676,6 +676,18 @@ int nzb_residual(const nzb_mesh* mesh, const nzb_physics* phys, int op, const do
   return dispatch(*mesh, *phys, w, (cudaStream_t)stream);
 }
 
+int nzb_observables(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_obs_args* args, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !args || !args->U || !args->bseg || !args->eseg || !args->out) return fail("observables: null argument");
+  if (args->n_seg <= 0) return fail("observables: no instances");
+  if (!mesh->edge_conn || !mesh->edge_geo || !mesh->area) return fail("observables: the mesh needs edge_conn, edge_geo and area");
+  if (!(args->r_gas > 0.0) || !(args->s_t > 0.0)) return fail("observables: r_gas and s_t must be positive");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const cudaError_t e = mesh->kind == NZB_TRI ? observables_launch_tri(*mesh, *phys, *args, st)
+                                              : observables_launch_quad(*mesh, *phys, *args, st);
+  return cuda_check(e, "observables launch");
+}
+
 int nzb_inverse_mass(const nzb_mesh* mesh, const double* R, double* out, void* stream) {
   if (check_mesh(mesh)) return -1;
   if (!R || !out) return fail("inverse_mass: null argument");

@@ -65,11 +65,42 @@ __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a) {
   for (int k = 0; k < N; ++k) r.d[k] = -a.d[k];
   return r;
 }
-// mixed with plain numbers
-template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, double b) { return a + Dual<N>(b); }
-template <int N> __device__ __forceinline__ Dual<N> operator+(double a, const Dual<N>& b) { return Dual<N>(a) + b; }
-template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, double b) { return a - Dual<N>(b); }
-template <int N> __device__ __forceinline__ Dual<N> operator-(double a, const Dual<N>& b) { return Dual<N>(a) - b; }
+// Mixed with plain numbers.  A plain operand has no derivative, and these
+// overloads skip the products with its zero derivative part outright: IEEE
+// arithmetic does not let the compiler drop x * 0.0 or x + 0.0 by itself.  The
+// values are the same as with a Dual of zero derivative.
+template <int N>
+__device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, double b) {
+  Dual<N> r;
+  r.v = a.v + b;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a.d[k];
+  return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator+(double a, const Dual<N>& b) {
+  Dual<N> r;
+  r.v = a + b.v;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = b.d[k];
+  return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, double b) {
+  Dual<N> r;
+  r.v = a.v - b;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a.d[k];
+  return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator-(double a, const Dual<N>& b) {
+  Dual<N> r;
+  r.v = a - b.v;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = -b.d[k];
+  return r;
+}
 template <int N>
 __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double b) {
   Dual<N> r;
@@ -78,9 +109,43 @@ __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double b) {
   for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * b;
   return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator*(double a, const Dual<N>& b) { return b * a; }
-template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double b) { return a / Dual<N>(b); }
-template <int N> __device__ __forceinline__ Dual<N> operator/(double a, const Dual<N>& b) { return Dual<N>(a) / b; }
+template <int N> __device__ __forceinline__ Dual<N> operator*(double a, const Dual<N>& b) {
+  Dual<N> r;
+  r.v = a * b.v;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a * b.d[k];
+  return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double b) {
+  Dual<N> r;
+  r.v = a.v / b;
+  const double inv = 1.0 / b;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * inv;
+  return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> operator/(double a, const Dual<N>& b) {
+  Dual<N> r;
+  r.v = a / b.v;
+  const double inv = 1.0 / b.v;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = -(r.v * b.d[k]) * inv;
+  return r;
+}
+
+// The type of an expression mixing A and B: Dual<N> when either is one.
+template <class A, class B>
+using Mix = decltype(*(A*)nullptr + *(B*)nullptr);
+template <class A, class B, class C>
+using Mix3 = Mix<Mix<A, B>, C>;
+
+// x's type holding the plain number v (a constant branch of a selection).
+template <class X>
+__device__ __forceinline__ X like(const X&, double v) {
+  return X(v);
+}
 
 #define NZB_DUAL_CMP(OP)                                                                                      \
   template <int N> __device__ __forceinline__ bool operator OP(const Dual<N>& a, const Dual<N>& b) {          \
@@ -114,6 +179,22 @@ __device__ __forceinline__ Dual<N> fmin(const Dual<N>& a, const Dual<N>& b) {
 template <int N>
 __device__ __forceinline__ Dual<N> fmax(const Dual<N>& a, const Dual<N>& b) {
   return b.v > a.v ? b : a;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> fmin(const Dual<N>& a, double b) {
+  return b < a.v ? Dual<N>(b) : a;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> fmin(double a, const Dual<N>& b) {
+  return b.v < a ? b : Dual<N>(a);
+}
+template <int N>
+__device__ __forceinline__ Dual<N> fmax(const Dual<N>& a, double b) {
+  return b > a.v ? Dual<N>(b) : a;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> fmax(double a, const Dual<N>& b) {
+  return b.v > a ? b : Dual<N>(a);
 }
 template <int N>
 __device__ __forceinline__ Dual<N> pow(const Dual<N>& a, double c) {

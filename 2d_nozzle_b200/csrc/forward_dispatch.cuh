@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "element.cuh"
+#include "observe.cuh"
 #include "slope.cuh"
 
 #ifndef NZB_INTERNAL
@@ -16,6 +17,10 @@ namespace nzb {
 
 NZB_INTERNAL cudaError_t element_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st);
 NZB_INTERNAL cudaError_t element_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st);
+NZB_INTERNAL cudaError_t observables_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a,
+                                                cudaStream_t st);
+NZB_INTERNAL cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a,
+                                                 cudaStream_t st);
 NZB_INTERNAL cudaError_t upload_tables_fwd_tri(const double* src, size_t count, size_t offset);
 NZB_INTERNAL cudaError_t upload_tables_fwd_quad(const double* src, size_t count, size_t offset);
 

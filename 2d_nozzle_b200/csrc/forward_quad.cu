@@ -59,6 +59,18 @@ cudaError_t element_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const 
   return cudaErrorInvalidValue;
 }
 
+cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a, cudaStream_t st) {
+  const unsigned nb = (unsigned)a.n_seg;
+  switch (m.order) {
+    case 0: k_observables<1, 0, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
+    case 1: k_observables<1, 1, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
+    case 2: k_observables<1, 2, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
+    case 3: k_observables<1, 3, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t upload_tables_fwd_quad(const double* src, size_t count, size_t offset) {
   return cudaMemcpyToSymbol(c_tab, src, sizeof(double) * count, sizeof(double) * offset);
 }

@@ -47,6 +47,14 @@ cudaError_t launch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cuda
   return cudaGetLastError();
 }
 
+template <int P>
+void observe(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a, cudaStream_t st) {
+  if (m.affine)
+    k_observables<0, P, true><<<(unsigned)a.n_seg, OBS_BT, 0, st>>>(m, ph, a);
+  else
+    k_observables<0, P, false><<<(unsigned)a.n_seg, OBS_BT, 0, st>>>(m, ph, a);
+}
+
 }  // namespace
 
 cudaError_t element_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
@@ -57,6 +65,17 @@ cudaError_t element_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const W
     case 3: return m.affine ? launch<0, 3, true>(m, ph, w, st) : launch<0, 3, false>(m, ph, w, st);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t observables_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a, cudaStream_t st) {
+  switch (m.order) {
+    case 0: observe<0>(m, ph, a, st); break;
+    case 1: observe<1>(m, ph, a, st); break;
+    case 2: observe<2>(m, ph, a, st); break;
+    case 3: observe<3>(m, ph, a, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t upload_tables_fwd_tri(const double* src, size_t count, size_t offset) {

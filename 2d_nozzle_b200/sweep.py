@@ -53,7 +53,7 @@ def build_instances(points, *, flux="hllc", tolerance=1e-10, max_iterations=200_
         except ShockInNozzle:
             refused.append(k)
             continue
-        instances.append(Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length))
+        instances.append(Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length, cs.geometry))
         index.append(k)
     return instances, index, refused
 

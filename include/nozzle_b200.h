@@ -360,6 +360,39 @@ int nzb_adjoint_create(int n_buckets, const nzb_mesh* meshes, const nzb_physics*
 int nzb_adjoint_run(nzb_adjoint* adjoint, int n_steps, void* stream);
 int nzb_adjoint_destroy(nzb_adjoint* adjoint);
 
+/* The integrals behind the parity observables of performance()
+ * (src/post/postprocess.py:56-75,155-192,193-255), per instance of a mesh or
+ * bucket, over the half channel that is meshed.  Boundary sums run over the
+ * face quadrature points with ds = w_q |dX/dsigma| and the owner-side trace;
+ * the entropy sum runs over the volume points with w_q det_q. */
+enum {
+  NZB_OBS_MOM_OUT = 0,   /* outflow  sum (rho vx vn + p nx) ds */
+  NZB_OBS_MOM_IN = 1,    /* inflow   the same */
+  NZB_OBS_WALL_PX = 2,   /* wall     sum p nx ds */
+  NZB_OBS_MASS_IN = 3,   /* inflow   sum rho vn ds */
+  NZB_OBS_MASS_OUT = 4,  /* outflow  the same */
+  NZB_OBS_EXIT_LEN = 5,  /* outflow  sum ds */
+  NZB_OBS_EXIT_MACH = 6, /* outflow  sum M ds */
+  NZB_OBS_EXIT_P = 7,    /* outflow  sum p ds */
+  NZB_OBS_EXIT_T = 8,    /* outflow  sum p / (R rho) ds */
+  NZB_OBS_ENTROPY = 9,   /* volume   sum (p rho^-gamma / s_t - 1)^2 w det */
+  NZB_OBS_AREA = 10,     /* sum of the element areas */
+  NZB_NOBS = 11
+};
+typedef struct {
+  const double* U;        /* (4, NP, E) state */
+  int32_t n_seg;          /* instances */
+  int32_t reserved;
+  const int32_t* bedges;  /* inflow, outflow and wall edges of every instance, grouped by instance */
+  const int32_t* bseg;    /* (n_seg + 1) offsets into bedges */
+  const int32_t* eseg;    /* (n_seg + 1) element offsets: instance i owns [eseg[i], eseg[i + 1]) */
+  double r_gas;           /* gas constant (exit temperature) */
+  double s_t;             /* p_t^(1 - gamma) (R T_t)^gamma (entropy reference) */
+  double* out;            /* (n_seg, NZB_NOBS) */
+} nzb_obs_args;
+/* All arrays device memory; one deterministic launch (fixed summation order). */
+int nzb_observables(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_obs_args* args, void* stream);
+
 const char* nzb_last_error(void);
 int nzb_version(void);
 

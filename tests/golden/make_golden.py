@@ -239,6 +239,37 @@ def config1():
     )
 
 
+PERF_FIELDS = ("thrust", "thrust_wall", "thrust_imbalance", "thrust_coefficient", "mass_flow_in", "mass_flow_out",
+               "mass_imbalance", "entropy_error", "exit_mach_area_averaged", "exit_pressure_ratio",
+               "exit_temperature_ratio", "specific_thrust", "specific_thrust_ratio", "discharge_coefficient",
+               "ideal_thrust", "thrust_efficiency")
+
+
+def observables():
+    """The reference's performance() of the tiny cases' states and of config 1's converged state."""
+    from types import SimpleNamespace
+
+    from src.api import build_case
+    from src.post.postprocess import performance
+
+    def perf(cs, U):
+        res = SimpleNamespace(operators=cs.operators, flow=cs.flow, U=U, geometry=cs.geometry)
+        pf = performance(res)
+        return {f: np.float64(getattr(pf, f)) for f in PERF_FIELDS}
+
+    arrays = {}
+    for kind, orders in (("tri", (0, 1, 2, 3)), ("quad", (1, 2, 3))):
+        for p in orders:
+            cs = build_case(contour="smooth", element=kind, order=p, refine=0)
+            U = np.load(os.path.join(HERE, f"tiny_{kind}_p{p}.npz"))["U"]
+            arrays.update({f"{kind}{p}_{k}": v for k, v in perf(cs, U).items()})
+    cs = build_case(contour="smooth", area_ratio=2.5, element="tri", order=1, refine=1, flux="roe",
+                    back_pressure_ratio=0.15)
+    U = np.load(os.path.join(HERE, "config1.npz"))["U_final"]
+    arrays.update({f"config1_{k}": v for k, v in perf(cs, U).items()})
+    _save("observables.npz", **arrays)
+
+
 def config3(n_steps=5):
     """Conical AR 3.0, p=3 quads, refine 3, HLLC, pb 0.6: fixed-step record."""
     from src.api import build_case
@@ -355,3 +386,5 @@ if __name__ == "__main__":
         sweep_outcomes()
     if "superbee" in which:
         superbee_cases()
+    if "observables" in which:
+        observables()

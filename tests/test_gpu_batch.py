@@ -24,7 +24,7 @@ def cases(tol=1e-8, max_it=6000, cfl=None):
     for el, p, r, ar, pb, contour in spec:
         flow = cfg.FlowConditions(flux="hllc", back_pressure_ratio=pb)
         cs = nz.build_case(element=el, order=p, refine=r, area_ratio=ar, contour=contour, flow=flow, options=opts)
-        out.append(pkg("batch").Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length))
+        out.append(pkg("batch").Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length, cs.geometry))
     return out
 
 
