@@ -119,7 +119,7 @@ class BatchSolver:
                 begin[i], end[i], local[i] = g_off + l_off, g_off + l_off + E_i, l_off
                 count[i] = 4.0 * E_i * ref.n_basis
                 f = instances[i].flow
-                tol[i] = opts0.tolerance * residual_scale(f, instances[i].length)
+                tol[i] = instances[i].opts.tolerance * residual_scale(f, instances[i].length)
                 p_back[i] = f.back_pressure
                 l_off += E_i
             self._keep.append(torch.as_tensor(elem_inst, device=dev))

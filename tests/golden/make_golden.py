@@ -322,6 +322,48 @@ def batch_cases():
     print("wrote batch_cases.json")
 
 
+CONTINUATION_CASES = [  # element, order, refine, area ratio, back pressure, contour, flux
+    ("tri", 2, 0, 2.5, 0.15, "smooth", "roe"),
+    ("tri", 3, 0, 2.0, 0.20, "bell", "hllc"),
+    ("quad", 1, 0, 2.5, 0.15, "smooth", "hllc"),
+]
+
+
+def continuation_cases():
+    """Solves with p-continuation (orders 0..p) at tolerance 1e-8, and the change_order projections."""
+    import json
+
+    from src.api import build_case, solve_nozzle
+    from src.post.postprocess import performance
+    from src.timestepping import initialize as ini
+
+    out = []
+    for el, p, r, ar, pb, contour, flux in CONTINUATION_CASES:
+        res = solve_nozzle(element=el, order=p, refine=r, area_ratio=ar, back_pressure_ratio=pb, contour=contour,
+                           flux=flux, tolerance=1e-8, max_iterations=30000, p_continuation=True, backend="numba",
+                           verbose=False)
+        row = {"case": [el, p, r, ar, pb, contour, flux], "converged": bool(res.converged),
+               "iterations": int(res.iterations), "residual": float(res.residual), "message": res.message}
+        if res.converged:
+            perf = performance(res)
+            row.update(thrust=perf.thrust, mass_flow_in=perf.mass_flow_in, exit_mach=perf.exit_mach_area_averaged)
+        out.append(row)
+    with open(os.path.join(HERE, "continuation_cases.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote continuation_cases.json")
+    # change_order of a quasi-1D state between every pair of orders (up and down)
+    arrays = {}
+    for kind in ("tri", "quad"):
+        cs = {q: build_case(contour="smooth", element=kind, order=q, refine=0) for q in (0, 1, 2, 3)}
+        for a in (0, 1, 2, 3):
+            U = np.asarray(ini.initial_state(cs[a].operators, cs[a].flow, cs[a].geometry, "quasi1d"))
+            arrays[f"{kind}_U{a}"] = U
+            for b in (0, 1, 2, 3):
+                if a != b:
+                    arrays[f"{kind}_{a}to{b}"] = np.asarray(ini.change_order(U, cs[a].operators, cs[b].operators))
+    _save("change_order.npz", **arrays)
+
+
 def _sweep_point(args):
     """One design point through the reference's own solve (one Numba thread per worker)."""
     k, el, p, r, ar, pb, max_it = args
@@ -388,3 +430,5 @@ if __name__ == "__main__":
         superbee_cases()
     if "observables" in which:
         observables()
+    if "continuation" in which:
+        continuation_cases()
