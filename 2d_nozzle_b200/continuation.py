@@ -97,13 +97,20 @@ def solve_case(cs, *, U0=None, device=None) -> ContinuationResult:
                               orders, its, prev)
 
 
+def _batch_key(inst):
+    f, o = inst.flow, inst.opts
+    return (f.gamma, f.flux, f.entropy_fix, f.hllc_low_mach, f.backflow, f.total_pressure, f.total_temperature,
+            f.Rgas, f.inflow_angle, o.replace(tolerance=0.0))
+
+
 def solve_batch(cases, *, warm_starts=None, device=None) -> list[ContinuationResult]:
     """Steady solves of many cases, one batched march per continuation stage.
 
     At stage k every case whose own order list has a k-th entry marches at that
-    order (below its target: to the transient tolerance), all of them in one
-    ``BatchSolver`` (the cases must share the march options, as any batch);
-    between stages each state is re-projected onto its next order.
+    order (below its target: to the transient tolerance), in one ``BatchSolver``
+    per group of cases that share the gas, the flux and the march options (any
+    batch's condition; back pressure and tolerance may differ); between stages
+    each state is re-projected onto its next order.
     """
     from .batch import BatchSolver, Instance
 
@@ -128,12 +135,18 @@ def solve_batch(cases, *, warm_starts=None, device=None) -> list[ContinuationRes
             ops_at[i] = ops
             insts.append(Instance(ops, cs.flow, stage_options(cs.options, order, targets[i]), U[i],
                                   float(cs.geometry.length), cs.geometry))
-        solver = BatchSolver(insts, device=device)
-        solver.run()
-        for i, r in zip(active, solver.results(with_state=True)):
-            U[i], prev[i] = r.U, ops_at[i]
-            its[i].append(r.iterations)
-            last[i] = r
-        del solver
+        # one batch per group of cases a batch can hold together: the same gas, flux and march
+        # options (back pressure and tolerance may differ per instance)
+        groups: dict = {}
+        for i, inst in zip(active, insts):
+            groups.setdefault(_batch_key(inst), []).append((i, inst))
+        for members in groups.values():
+            solver = BatchSolver([inst for _, inst in members], device=device)
+            solver.run()
+            for (i, _), r in zip(members, solver.results(with_state=True)):
+                U[i], prev[i] = r.U, ops_at[i]
+                its[i].append(r.iterations)
+                last[i] = r
+            del solver
     return [ContinuationResult(U[i], last[i].converged, int(sum(its[i])), float(last[i].residual), last[i].status,
                                "", orders[i], its[i], prev[i]) for i in range(n)]

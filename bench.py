@@ -13,8 +13,9 @@ other point is marched from its quasi-1D initial state, all together, each to
 its own retirement (converged, stalled, diverged, non-finite or the iteration
 cap).  ``value`` counts converged solves per second with every state resident
 in HBM; ``e2e`` times the public path -- BatchSolver set-up from host arrays
-(states, geometry, connectivity copied in), the march, and every state and
-status copied back.  ``plain`` marches a subset one instance at a time through
+(states, geometry, connectivity copied in), the march, every status and each
+point's performance() metrics (thrust, mass flows, exit averages, entropy
+error: integrated on the device, only the sums copied back).  ``plain`` marches a subset one instance at a time through
 the single-solve backend and the same subset as a batch: their ratio is the
 batched speed-up over the same attempted set.
 
@@ -364,6 +365,43 @@ def adjoint_section(args, torch):
     n_plain = sum(g is not None for g in plain.values())
     diff = max([abs(out[i].grad[k] - g[k]) / max(abs(g[k]), 1e-12) for i, g in plain.items() for k in names
                 if g is not None and out[i].grad is not None] or [0.0])
+
+    # every member one at a time, estimated: a plain member costs its forward iterations times the plain
+    # forward march's cost per iteration, its adjoint iterations times the plain adjoint march's, plus a
+    # fixed set-up (case build, seeds, coordinate products) taken from the measured subset; the iteration
+    # counts are the batch's own, which equal the plain ones
+    batch = pkg("batch")
+    cs0 = dc.case_at(members[0])
+    inst0 = batch.Instance(cs0.operators, cs0.flow, dc.options, cs0.initial_state(), float(cs0.geometry.length))
+    bk, U0, _ = plain_solve(inst0, torch)
+    ci = dc.options.check_interval
+    bk._S[0].copy_(U0)
+    bk.run_device(1)
+    bk.run_device(ci)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        bk.run_device(ci)
+        float(bk._res.item())
+    t_fwd = (time.perf_counter() - t0) / (10 * ci)
+    model = ad.AdjointModel(cs0.operators, cs0.flow, dc.options)
+    U_soa = ad.to_soa(torch.as_tensor(np.asarray(cs0.initial_state()), device="cuda"))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0)
+    am = ad.AdjointMarch(model, U_soa, torch.randn(U_soa.shape, generator=gen, dtype=torch.float64, device="cuda"),
+                         dc.options.cfl)
+    am._create(1e-300, 10**9)
+    am.run(0)
+    am.run(100)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        am.run(100)
+    t_adj = (time.perf_counter() - t0) / 500
+    del am, bk
+    cost = lambda r: r.forward_iterations * t_fwd + r.adjoint_iterations * t_adj  # noqa: E731
+    fixed = max(0.0, (t_plain - sum(cost(out[i]) for i in sub)) / len(sub))
+    est_all = sum(cost(r) for r in out) + fixed * len(out)
     return {"workload": f"{len(members)} bezier8 members (8 offsets, sigma 2% of the throat half-height, seed 0) "
                         f"around AR 2.5, tri p=2 refine 2 (2240 elements), AUSM+-up, forward and adjoint to 1e-10",
             "metric": "thrust gradients/s (8 design variables each)", "batched_gradients": len(ok),
@@ -374,7 +412,11 @@ def adjoint_section(args, torch):
             "forward_iterations_max": max(r.forward_iterations for r in out),
             "max_rel_diff_batched_vs_plain": diff, "batched_phases_s": bg.timings,
             "forward_status": {st: sum(r.forward_status == st for r in out) for st in {r.forward_status for r in out}},
-            "forward_iteration_cap": args.adjoint_cap}
+            "forward_iteration_cap": args.adjoint_cap,
+            "all_members_estimated_plain_seconds": est_all,
+            "speedup_all_members": (len(ok) / t_batch) / max(len(ok) / est_all, 1e-300),
+            "plain_cost_model": {"forward_s_per_iteration": t_fwd, "adjoint_s_per_iteration": t_adj,
+                                 "fixed_s_per_member": fixed}}
 
 
 def run_ours(args, rank, world, torch, dist):
@@ -430,13 +472,15 @@ def run_ours(args, rank, world, torch, dist):
         t0 = time.perf_counter()
         sv = BatchSolver(insts)
         sv.run()
-        out = sv.results(with_state=True)
+        out = sv.results(with_state=False)
+        perf = sv.observables()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         if k > 0:
             e2e_t.append(t1 - t0)
         h2d = sv.h2d_bytes
-        d2h = sum(o.U.nbytes for o in out) + 4 * 2 * len(out) + 8 * 2 * len(out) + 4 * sv.chunks
+        # statuses, iterations, residuals, the observable sums, and one 4-byte read per chunk
+        d2h = (4 * 2 + 8 * 2) * len(out) + 8 * pkg("capi").NOBS * len(perf) + 4 * sv.chunks
         del sv
     e2e_value = world * n_conv / float(np.mean(e2e_t))
 
@@ -523,7 +567,7 @@ def run_ours(args, rank, world, torch, dist):
                    "converged_per_step": int(n_conv), "l2": "flushed (256 MB write) before each sweep",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": "BatchSolver(host instances) -> run() -> results(with_state=True)"},
+                "path": "BatchSolver(host instances) -> run() -> results() + observables()"},
         "plain": plain,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
