@@ -35,7 +35,7 @@ from . import capi
 from . import nozzle as nz
 from .backend import B200Backend
 from .config import SolverOptions, step_coefficient
-from .layout import DeviceMesh, physics_struct
+from .layout import DeviceMesh, face_tangent_table, physics_struct
 from .march import solve as march_solve
 from .mesh import INFLOW, OUTFLOW
 from .operators import build_operators
@@ -43,16 +43,6 @@ from .operators import build_operators
 OBJECTIVES = ("thrust", "thrust_coefficient", "exit_mach", "mass_flow", "exit_pressure")
 FLOW_DESIGN_PARAMETERS = ("back_pressure",)
 STATUS = {0: "running", 1: "converged", 2: "non-finite", 5: "max_iterations"}
-
-
-def face_tangent_table(ref) -> np.ndarray:
-    """(4, 4): the tangent of face f is sum_v T[f, v] X_v (straight faces, vertex geometry)."""
-    d = np.asarray(ref.dgeom_dsigma_face)  # (NF, NV, NQF)
-    if np.abs(d - d[:, :, :1]).max() > 0.0:
-        raise NotImplementedError("the coordinate adjoint takes straight-sided elements")
-    out = np.zeros((4, 4))
-    out[: d.shape[0], : d.shape[1]] = d[:, :, 0]
-    return out
 
 
 def to_soa(U):
@@ -100,10 +90,12 @@ class AdjointModel:
         if X is None or (X.shape == self.X0.shape and torch.allclose(X.detach().to(self.device), self.X0,
                                                                      rtol=1e-14, atol=1e-15)):
             return self.mesh
-        Xh = X.detach().cpu().numpy()
-        if self._other[0] is None or not np.array_equal(self._other[0], Xh):
-            ops = build_operators(self.ops.topology, Xh, self.ops.ref.order)
-            self._other = (Xh.copy(), DeviceMesh(ops, self.device))
+        # the metric terms at X are rebuilt on the device (nzb_geometry); the connectivity is this mesh's
+        Xd = X.detach().to(device=self.device, dtype=torch.float64)
+        if self._other[0] is None or not torch.equal(self._other[0], Xd):
+            mesh = self._other[1] if self._other[1] is not None else DeviceMesh(self.ops, self.device)
+            mesh.set_geometry(Xd, self.elem_nodes_t)
+            self._other = (Xd.clone(), mesh)
         return self._other[1]
 
     def verts(self, X):

@@ -193,6 +193,19 @@ class ObsArgs(C.Structure):
     ]
 
 
+class GeometryArgs(C.Structure):
+    _fields_ = [
+        ("X", P),
+        ("elem_nodes", P),
+        ("edge_conn", P),
+        ("dgs", C.c_double * 16),
+        ("geo", P),
+        ("minv", P),
+        ("area", P),
+        ("edge_geo", P),
+    ]
+
+
 # column of each per-instance sum of nzb_observables
 (OBS_MOM_OUT, OBS_MOM_IN, OBS_WALL_PX, OBS_MASS_IN, OBS_MASS_OUT, OBS_EXIT_LEN, OBS_EXIT_MACH, OBS_EXIT_P,
  OBS_EXIT_T, OBS_ENTROPY, OBS_AREA) = range(11)
@@ -209,6 +222,7 @@ SIGNATURES = [
     ("nzb_residual", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.c_int, P, P, P, P]),
     ("nzb_inverse_mass", C.c_int, [C.POINTER(Mesh), P, P, P]),
     ("nzb_observables", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(ObsArgs), P]),
+    ("nzb_geometry", C.c_int, [C.POINTER(Mesh), C.POINTER(GeometryArgs), P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

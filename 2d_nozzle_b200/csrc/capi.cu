@@ -688,6 +688,20 @@ int nzb_observables(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_obs
   return cuda_check(e, "observables launch");
 }
 
+int nzb_geometry(const nzb_mesh* mesh, const nzb_geometry_args* args, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!args || !args->X || !args->elem_nodes || !args->edge_conn || !args->geo || !args->area || !args->edge_geo)
+    return fail("geometry: null argument");
+  if (!mesh->affine && !args->minv) return fail("geometry: general geometry needs minv");
+  if (mesh->n_edge <= 0) return fail("geometry: the mesh has no edges");
+  if ((mesh->n_elem + 127) / 128 > 0x7fffffff || (mesh->n_edge + 127) / 128 > 0x7fffffff)
+    return fail("geometry: too many elements or edges for one launch");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const cudaError_t e = mesh->kind == NZB_TRI ? geometry_launch_tri(*mesh, *args, st)
+                                              : geometry_launch_quad(*mesh, *args, st);
+  return cuda_check(e, "geometry launch");
+}
+
 int nzb_inverse_mass(const nzb_mesh* mesh, const double* R, double* out, void* stream) {
   if (check_mesh(mesh)) return -1;
   if (!R || !out) return fail("inverse_mass: null argument");

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "element.cuh"
+#include "geometry.cuh"
 #include "observe.cuh"
 #include "slope.cuh"
 
@@ -21,6 +22,8 @@ NZB_INTERNAL cudaError_t observables_launch_tri(const nzb_mesh& m, const nzb_phy
                                                 cudaStream_t st);
 NZB_INTERNAL cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a,
                                                  cudaStream_t st);
+NZB_INTERNAL cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
+NZB_INTERNAL cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t upload_tables_fwd_tri(const double* src, size_t count, size_t offset);
 NZB_INTERNAL cudaError_t upload_tables_fwd_quad(const double* src, size_t count, size_t offset);
 

@@ -47,6 +47,13 @@ cudaError_t launch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cuda
   return cudaGetLastError();
 }
 
+template <int P>
+void geometry(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
+  const unsigned ne = (unsigned)((m.n_elem + 127) / 128), nk = (unsigned)((m.n_edge + 127) / 128);
+  k_elem_geometry<1, P, false><<<ne, 128, 0, st>>>(m, a);
+  k_edge_geometry<1, P><<<nk, 128, 0, st>>>(m, a);
+}
+
 }  // namespace
 
 cudaError_t element_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
@@ -66,6 +73,17 @@ cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_physics& ph, co
     case 1: k_observables<1, 1, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
     case 2: k_observables<1, 2, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
     case 3: k_observables<1, 3, false><<<nb, OBS_BT, 0, st>>>(m, ph, a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
+  switch (m.order) {
+    case 0: geometry<0>(m, a, st); break;
+    case 1: geometry<1>(m, a, st); break;
+    case 2: geometry<2>(m, a, st); break;
+    case 3: geometry<3>(m, a, st); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -55,6 +55,16 @@ void observe(const nzb_mesh& m, const nzb_physics& ph, const nzb_obs_args& a, cu
     k_observables<0, P, false><<<(unsigned)a.n_seg, OBS_BT, 0, st>>>(m, ph, a);
 }
 
+template <int P>
+void geometry(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
+  const unsigned ne = (unsigned)((m.n_elem + 127) / 128), nk = (unsigned)((m.n_edge + 127) / 128);
+  if (m.affine)
+    k_elem_geometry<0, P, true><<<ne, 128, 0, st>>>(m, a);
+  else
+    k_elem_geometry<0, P, false><<<ne, 128, 0, st>>>(m, a);
+  k_edge_geometry<0, P><<<nk, 128, 0, st>>>(m, a);
+}
+
 }  // namespace
 
 cudaError_t element_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cudaStream_t st) {
@@ -73,6 +83,17 @@ cudaError_t observables_launch_tri(const nzb_mesh& m, const nzb_physics& ph, con
     case 1: observe<1>(m, ph, a, st); break;
     case 2: observe<2>(m, ph, a, st); break;
     case 3: observe<3>(m, ph, a, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
+  switch (m.order) {
+    case 0: geometry<0>(m, a, st); break;
+    case 1: geometry<1>(m, a, st); break;
+    case 2: geometry<2>(m, a, st); break;
+    case 3: geometry<3>(m, a, st); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -110,6 +110,16 @@ def physics_struct(flow, opts, ref) -> capi.Physics:
     return ph
 
 
+def face_tangent_table(ref) -> np.ndarray:
+    """(4, 4): the tangent of face f is sum_v T[f, v] X_v (straight faces, vertex geometry)."""
+    d = np.asarray(ref.dgeom_dsigma_face)  # (NF, NV, NQF)
+    if np.abs(d - d[:, :, :1]).max() > 0.0:
+        raise NotImplementedError("the device geometry takes straight-sided elements")
+    out = np.zeros((4, 4))
+    out[: d.shape[0], : d.shape[1]] = d[:, :, 0]
+    return out
+
+
 def host_arrays(ops, *, force_general: bool = False) -> dict:
     """The per-element / per-edge arrays of one mesh, in device (structure-of-arrays) layout."""
     ref = ops.ref
@@ -233,6 +243,32 @@ class DeviceMesh:
         m.lim_scale = self.lim_scale.data_ptr()
         self.c = m
         self.c_ref = C.byref(m)
+
+    def set_geometry(self, X, elem_nodes) -> None:
+        """Rebuild this mesh's metric terms on the device from node coordinates (``nzb_geometry``).
+
+        ``X`` (n_node, 2) and ``elem_nodes`` (E, NV) vertex ids, host or device
+        arrays; the connectivity stays.  Queued on the current stream.
+        """
+        torch = self.torch
+        Xd = torch.as_tensor(X, dtype=torch.float64, device=self.device).contiguous()
+        en = torch.as_tensor(np.ascontiguousarray(elem_nodes) if isinstance(elem_nodes, np.ndarray) else elem_nodes,
+                             device=self.device).to(torch.int32).contiguous()
+        if en.ndim != 2 or en.shape[0] != self.E or en.shape[1] != self.nf or Xd.ndim != 2 or Xd.shape[1] != 2:
+            raise ValueError("set_geometry takes X (n_node, 2) and elem_nodes (E, NV)")
+        if "edge_conn" not in self.arrays:
+            raise ValueError("set_geometry needs the mesh's edge connectivity")
+        a = capi.GeometryArgs()
+        a.X, a.elem_nodes, a.edge_conn = Xd.data_ptr(), en.data_ptr(), self.arrays["edge_conn"].data_ptr()
+        for k, v in enumerate(face_tangent_table(self.ref).ravel()):
+            a.dgs[k] = float(v)
+        a.geo, a.area, a.edge_geo = (self.arrays[k].data_ptr() for k in ("geo", "area", "edge_geo"))
+        a.minv = self.arrays["minv"].data_ptr() if "minv" in self.arrays else None
+        capi.check(capi.load().nzb_geometry(self.c_ref, C.byref(a), self.stream()), "nzb_geometry")
+        self._geometry_inputs = (Xd, en)  # alive until the queued kernels have read them
+        if getattr(self, "elem_share", None) is not None:
+            area = self.arrays["area"]
+            self.elem_share.copy_(area / area.sum())
 
     @property
     def edge_pass(self) -> bool:

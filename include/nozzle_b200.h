@@ -393,6 +393,24 @@ typedef struct {
 /* All arrays device memory; one deterministic launch (fixed summation order). */
 int nzb_observables(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_obs_args* args, void* stream);
 
+/* The metric terms of a mesh from its node coordinates, on the device: the
+ * coordinate-dependent part of build_operators (src/spatial/operators.py:
+ * 240-303) for straight-sided elements.  mesh supplies kind, order, affine,
+ * n_elem and n_edge; the outputs are the arrays an nzb_mesh points to (they may
+ * be the mesh's own).  dgs is as for nzb_vjp_coords (host memory, copied into
+ * the kernel's parameters).  All other arrays device memory. */
+typedef struct {
+  const double* X;           /* (n_node, 2) node coordinates */
+  const int32_t* elem_nodes; /* (E, NV) vertex node ids, NV = 3 triangles, 4 quads */
+  const int32_t* edge_conn;  /* (3, n_edge) as in nzb_mesh: owner, neighbour, owner face in bits 0-2 */
+  double dgs[16];            /* tangent of face f = sum_v dgs[4 f + v] X_v */
+  double* geo;               /* out: affine (5, E) xi_x, xi_y, eta_x, eta_y, det; else (2 NV, E) vertex x then y */
+  double* minv;              /* out, general geometry only: (NP * NP, E) inverse mass matrices */
+  double* area;              /* out: (E) */
+  double* edge_geo;          /* out: (n_edge, 4) unit normal, |dX/dsigma|, length */
+} nzb_geometry_args;
+int nzb_geometry(const nzb_mesh* mesh, const nzb_geometry_args* args, void* stream);
+
 const char* nzb_last_error(void);
 int nzb_version(void);
 

@@ -63,6 +63,7 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(capi.AdjointBuffers) == 9 * 8
     assert ctypes.sizeof(capi.AdjointMarch) == 8 + 9 * 8 + 8 + 2 * 4
     assert ctypes.sizeof(capi.ObsArgs) == 8 + 2 * 4 + 3 * 8 + 2 * 8 + 8
+    assert ctypes.sizeof(capi.GeometryArgs) == 3 * 8 + 16 * 8 + 4 * 8
 
 
 def test_lebesgue_constant_bounds_probe_values():
