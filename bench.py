@@ -420,6 +420,62 @@ def adjoint_section(args, torch):
                                  "fixed_s_per_member": fixed}}
 
 
+def vjp_micro(torch, n_members=64):
+    """Adjoint-kernel microbenchmark (profiling): the batched-gradient bucket -- n_members bezier8 members,
+    tri p = 2, refine 2, AUSM+-up, 2240 elements each -- after 50 batched forward steps; k_vjp per launch
+    in product and RK4-stage modes beside the residual kernel, with a random adjoint state."""
+    import ctypes as C
+
+    ad, capi = pkg("adjoint"), pkg("capi")
+    dc = ad.differentiable_case(contour="bezier8", area_ratio=2.5, order=2, refine=2, flux="ausmup",
+                                back_pressure_ratio=0.15, tolerance=1e-10)
+    members = bezier8_members(n_members)
+    bg = ad.BatchGradient(dc, members, "thrust", names=tuple(members[0]))
+    sv = pkg("batch").BatchSolver(bg.instances)
+    sv.step_chunk(1, True)
+    sv.step_chunk(50, False)
+    dm, S0, ph = sv.meshes[0], sv.buffers[0][1][0], sv.phys[0]
+    lib, st = capi.load(), torch.cuda.current_stream()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0)
+    rnd = lambda: torch.randn(S0.shape, generator=gen, dtype=torch.float64, device="cuda")  # noqa: E731
+    lam, seed, out = rnd(), rnd(), torch.empty_like(S0)
+    lam0, f0, f1, f2 = lam.clone(), torch.zeros_like(S0), torch.zeros_like(S0), torch.zeros_like(S0)
+    dt = torch.full((dm.E,), 1e-4, dtype=torch.float64, device="cuda")
+    wave = torch.empty(dm.E, dtype=torch.float64, device="cuda")
+    status = torch.zeros(n_members, dtype=torch.int32, device="cuda")
+    mesh = capi.Mesh()
+    C.memmove(C.byref(mesh), C.byref(dm.c), C.sizeof(capi.Mesh))
+    mesh.inst_status = status.data_ptr()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timeit(fn, n=20):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            ev[0].record(st)
+            fn()
+            ev[1].record(st)
+            torch.cuda.synchronize()
+            ts.append(ev[0].elapsed_time(ev[1]) * 1e3)
+        return float(np.median(ts))
+
+    res = {"workload": f"batched-gradient bucket: {n_members} bezier8 members, tri p=2 refine 2, {dm.E} elements, AUSM+-up",
+           "unit": "us per launch"}
+    a = capi.AdjointArgs()
+    a.mode, a.U, a.lam, a.seed, a.out = capi.ADJ_VJP, S0.data_ptr(), lam.data_ptr(), seed.data_ptr(), out.data_ptr()
+    res["k_vjp_product"] = timeit(lambda: capi.check(lib.nzb_vjp(C.byref(mesh), C.byref(ph), C.byref(a), st.cuda_stream), "nzb_vjp"))
+    r = capi.AdjointArgs()
+    r.mode, r.stage = capi.ADJ_RK4, 1
+    r.U, r.lam, r.seed, r.out, r.lam0, r.dt = (t.data_ptr() for t in (S0, lam, seed, out, lam0, dt))
+    r.f0, r.f1, r.f2 = f0.data_ptr(), f1.data_ptr(), f2.data_ptr()
+    res["k_vjp_rk4_stage"] = timeit(lambda: capi.check(lib.nzb_vjp(C.byref(mesh), C.byref(ph), C.byref(r), st.cuda_stream), "nzb_vjp"))
+    res["k_element_residual"] = timeit(lambda: capi.check(lib.nzb_residual(C.byref(mesh), C.byref(ph), 0, S0.data_ptr(), out.data_ptr(),
+                                                                           wave.data_ptr(), st.cuda_stream), "nzb_residual"))
+    return res
+
+
 def run_ours(args, rank, world, torch, dist):
     capi = pkg("capi")
     BatchSolver = pkg("batch").BatchSolver
@@ -644,6 +700,7 @@ def main():
     ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
     ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
     ap.add_argument("--micro-nr", type=int, default=500, help="microbench cells across")
+    ap.add_argument("--vjp-only", action="store_true", help="run only the adjoint-kernel microbench (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -663,6 +720,9 @@ def main():
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_mod
     pkg("build").build()
+    if args.vjp_only:
+        print(json.dumps(vjp_micro(torch)))
+        return
     if args.micro_only:
         peak, kind = load_peaks()
         print(json.dumps(microbench(torch, pkg("capi"), pkg("backend").B200Backend, pkg("config"), peak, kind,
