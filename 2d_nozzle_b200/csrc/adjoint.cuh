@@ -125,6 +125,24 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, NZB_MINB_VJP * 128 / Launch<
   if (active) {
     const double* __restrict__ U = w.U;
     const double* __restrict__ L = w.lam;
+    // the epilogue's operands (dJ/dU, the step's starting lambda, in the last
+    // RK4 stage the stored stage rates) start toward the caches now, so the
+    // loads after the face and volume loops need not wait on DRAM
+    if (w.mode != ADJ_VJP) {
+#pragma unroll
+      for (int k = 0; k < NP * 4; ++k) {
+        const int64_t o = (int64_t)k * E + e;
+        prefetch_line(w.seed + o);
+        if (w.mode == ADJ_RK4) {
+          prefetch_line(w.lam0 + o);
+          if (w.stage == 3) {
+            prefetch_line(w.f0 + o);
+            prefetch_line(w.f1 + o);
+            prefetch_line(w.f2 + o);
+          }
+        }
+      }
+    }
 #pragma unroll
     for (int i = 0; i < NP * 4; ++i) vacc[i * BT + t] = 0.0;
     double xx = 0, xy = 0, yx = 0, yy = 0, det = 1.0;

@@ -319,6 +319,10 @@ __device__ __forceinline__ void block_sum_store(double v, double* dst) {
   }
 }
 
+// Start a global cache line toward L2; no register holds it.  The adjoint
+// kernel issues these at entry for operands it reads only in its epilogue.
+__device__ __forceinline__ void prefetch_line(const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Threads per block: 128, or 64 where the per-thread face accumulator would
 // push static shared memory past 48 KB (cubic quadrilaterals).
 //
