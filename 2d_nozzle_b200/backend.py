@@ -33,7 +33,7 @@ from .layout import DeviceMesh, physics_struct
 class B200Backend:
     name = "b200"
 
-    def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False):
+    def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False, device_metrics: bool = False):
         import torch
 
         self.torch = torch
@@ -50,7 +50,9 @@ class B200Backend:
         self.component_weight = np.array([1.0, 1.0 / a_t, 1.0 / a_t, 1.0 / a_t**2]).reshape(1, 1, 4)
 
         self.lib = capi.load()
-        self.mesh = DeviceMesh(ops, device, force_general=force_general)
+        # device_metrics: operators built without inverse mass matrices (lean) get their metric
+        # terms from the node coordinates on the device
+        self.mesh = DeviceMesh(ops, device, force_general=force_general, device_metrics=device_metrics)
         self.phys = physics_struct(flow, opts, ops.ref)
         self._phys_ref = capi.C.byref(self.phys)
         d = self.mesh.device

@@ -62,13 +62,27 @@ __device__ __forceinline__ double pfe(int side, int f, int j, int q) {
   return c_tab[S::O_PFE + ((side * S::NF + f) * S::NE + j) * S::NQF + q];
 }
 
+// An element's coefficients as the limiter reads and writes them: a register
+// array, or this thread's column of a shared-memory block (stride BT), where a
+// kernel keeps them to leave registers free.
+template <int NP>
+struct RegCoef {
+  double (&u)[NP][4];
+  __device__ __forceinline__ double& operator()(int i, int s) const { return u[i][s]; }
+};
+template <int BT>
+struct SmemCoef {
+  double* col;  // &block[t]
+  __device__ __forceinline__ double& operator()(int i, int s) const { return col[(i * 4 + s) * BT]; }
+};
+
 // One probe point of this element's solution: volume point pt < NQV, else the
 // element's own trace at face point (f, q), with the basis of its side of that
 // face (bit f of sides), as the reference's probe set (src/spatial/limiter.py:
 // 78-95).  pt is the same on every lane of a warp (the loops over points are
 // rolled), so the table reads are constant-cache broadcasts.
-template <int K, int P>
-__device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4], int pt, int sides, double (&w)[4]) {
+template <int K, int P, class A>
+__device__ __forceinline__ void probe_point(const A& u, int pt, int sides, double (&w)[4]) {
   using S = Shape<K, P>;
   w[0] = w[1] = w[2] = w[3] = 0.0;
   if (pt < S::NQV) {
@@ -76,7 +90,7 @@ __device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4
     for (int i = 0; i < S::NP; ++i) {
       const double phi = c_tab[S::O_PHI + i * S::NQV + pt];
 #pragma unroll
-      for (int s = 0; s < 4; ++s) w[s] = fma(phi, u[i][s], w[s]);
+      for (int s = 0; s < 4; ++s) w[s] = fma(phi, u(i, s), w[s]);
     }
   } else {
     const int f = (pt - S::NQV) / S::NQF, q = (pt - S::NQV) - f * S::NQF;
@@ -91,7 +105,7 @@ __device__ __forceinline__ void probe_point(const double (&u)[Shape<K, P>::NP][4
         if (ff == f) {
           const int nn = edge_node(K, P, ff, j);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) v[s] = u[nn][s];
+          for (int s = 0; s < 4; ++s) v[s] = u(nn, s);
         }
       }
 #pragma unroll
@@ -107,8 +121,8 @@ __device__ __forceinline__ double pressure_at(const double (&w)[4], double g) {
 
 // Minimum pressure over the probe set of ubar + theta (u - ubar), through the
 // reference's scaling formula (src/spatial/limiter.py:146-148,151-178).
-template <int K, int P>
-__device__ __forceinline__ double pmin_at(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4], double theta,
+template <int K, int P, class A>
+__device__ __forceinline__ double pmin_at(const A& u, const double (&ub)[4], double theta,
                                           int sides, double g) {
   double pmin = 1e300;
 #pragma unroll 1
@@ -128,8 +142,8 @@ __device__ __forceinline__ double pmin_at(const double (&u)[Shape<K, P>::NP][4],
 // at which p(ubar + t (w - ubar)) = eps_p at some point w.  Along the segment
 // h(t) = rho(t) (p(t) - eps_p) / (gamma - 1) = a t^2 + b t + c with
 // h(0) = rho_bar (p_bar - eps_p) / (gamma - 1) > 0; t* = 1e300 when no point binds.
-template <int K, int P>
-__device__ __forceinline__ void probe_scan(const double (&u)[Shape<K, P>::NP][4], const double (&ub)[4], int sides,
+template <int K, int P, class A>
+__device__ __forceinline__ void probe_scan(const A& u, const double (&ub)[4], int sides,
                                            double eps_p, double g, double& rmin, double& pmin, double& tstar) {
   const double e1 = eps_p / (g - 1.0);
   const double c = ub[3] * ub[0] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) - e1 * ub[0];
@@ -211,8 +225,8 @@ __device__ __forceinline__ void mean_weights(const nzb_mesh& m, int64_t e, doubl
 // Zhang-Shu positivity limiter of one element, in place
 // (src/spatial/limiter.py:103-243; the O(NP) Lebesgue screen of
 // src/backends/_numba_kernels.py:1010-1026 skips provably admissible elements).
-template <int K, int P, bool AFF>
-__device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], const nzb_mesh& m,
+template <int K, int P, bool AFF, class A>
+__device__ __forceinline__ void limit_element(const A& u, const nzb_mesh& m,
                                               const nzb_physics& ph, int64_t e, int sides, int& scaled,
                                               int& repaired) {
   using S = Shape<K, P>;
@@ -224,7 +238,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
 #pragma unroll
   for (int i = 0; i < S::NP; ++i)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u[i][s], ub[s]);
+    for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u(i, s), ub[s]);
 
   // last-resort repair of a non-physical cell average
   const double rho_new = ub[0] < ph.rho_floor ? ph.rho_floor : ub[0];
@@ -234,8 +248,8 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
     const double d0 = rho_new - ub[0], d3 = rhoE_new - ub[3];
 #pragma unroll
     for (int i = 0; i < S::NP; ++i) {
-      u[i][0] += d0;
-      u[i][3] += d3;
+      u(i, 0) += d0;
+      u(i, 3) += d3;
     }
     repaired = 1;
 #pragma unroll
@@ -243,7 +257,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
 #pragma unroll
     for (int i = 0; i < S::NP; ++i)
 #pragma unroll
-      for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u[i][s], ub[s]);
+      for (int s = 0; s < 4; ++s) ub[s] = fma(mw[i], u(i, s), ub[s]);
   }
   const double pbar = (g - 1.0) * (ub[3] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / ub[0]);
   double eps_r = ph.lim_fraction * ub[0];
@@ -256,7 +270,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
 #pragma unroll
   for (int i = 0; i < S::NP; ++i)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) dev[s] = fmax(dev[s], fabs(u[i][s] - ub[s]));
+    for (int s = 0; s < 4; ++s) dev[s] = fmax(dev[s], fabs(u(i, s) - ub[s]));
   const double lam = ph.lebesgue;
   const double rho_lo = ub[0] - lam * dev[0];
   if (rho_lo >= eps_r) {
@@ -300,7 +314,7 @@ __device__ __forceinline__ void limit_element(double (&u)[Shape<K, P>::NP][4], c
 #pragma unroll
   for (int i = 0; i < S::NP; ++i)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) u[i][s] = ub[s] + theta * (u[i][s] - ub[s]);
+    for (int s = 0; s < 4; ++s) u(i, s) = ub[s] + theta * (u(i, s) - ub[s]);
   scaled = 1;
 }
 
@@ -452,7 +466,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
     for (int i = 0; i < NP; ++i)
 #pragma unroll
       for (int s = 0; s < 4; ++s) u[i][s] = w.V[(s * NP + i) * E + e];
-    if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(u, m, ph, e, face_sides<K, P>(m, e), scaled, repaired);
+    if (ph.limiter == 1 && P > 0)
+      limit_element<K, P, AFF>(RegCoef<NP>{u}, m, ph, e, face_sides<K, P>(m, e), scaled, repaired);
 #pragma unroll
     for (int i = 0; i < NP; ++i)
 #pragma unroll
@@ -719,21 +734,22 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
       }
       if (stage) {
         if (w.elem_norm && w.stage == 1) w.elem_norm[e] = nrm;
-        double ul[NP][4];
+        // the limiter works where the new state is: this thread's shared-memory
+        // column (USM) or the registers -- no copy, no spilled array
+        if constexpr (USM) {
+          const SmemCoef<BT> col{facc + t};
+          if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(col, m, ph, e, sides, scaled, repaired);
 #pragma unroll
-        for (int i = 0; i < NP; ++i)
+          for (int i = 0; i < NP; ++i)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            if constexpr (USM)
-              ul[i][s] = facc[(i * 4 + s) * BT + t];
-            else
-              ul[i][s] = u[i][s];
-          }
-        if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(ul, m, ph, e, sides, scaled, repaired);
+            for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = col(i, s);
+        } else {
+          if (ph.limiter == 1 && P > 0) limit_element<K, P, AFF>(RegCoef<NP>{u}, m, ph, e, sides, scaled, repaired);
 #pragma unroll
-        for (int i = 0; i < NP; ++i)
+          for (int i = 0; i < NP; ++i)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = ul[i][s];
+            for (int s = 0; s < 4; ++s) w.out[(s * NP + i) * E + e] = u[i][s];
+        }
         if (w.flags) w.flags[e] = (uint8_t)(scaled | (repaired << 1));
       }
     }

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128) k_superbee(const nzb_mesh m, const nzb_ph
         changed |= v != u[i][s];
         u[i][s] = v;
       }
-    limit_element<K, P, AFF>(u, m, ph, e, sides, scaled, repaired);
+    limit_element<K, P, AFF>(RegCoef<NP>{u}, m, ph, e, sides, scaled, repaired);
     scaled |= changed ? 1 : 0;
 #pragma unroll
     for (int i = 0; i < NP; ++i)

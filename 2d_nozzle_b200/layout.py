@@ -120,8 +120,13 @@ def face_tangent_table(ref) -> np.ndarray:
     return out
 
 
-def host_arrays(ops, *, force_general: bool = False) -> dict:
-    """The per-element / per-edge arrays of one mesh, in device (structure-of-arrays) layout."""
+def host_arrays(ops, *, force_general: bool = False, device_metrics: bool = False) -> dict:
+    """The per-element / per-edge arrays of one mesh, in device (structure-of-arrays) layout.
+
+    ``device_metrics``: general geometry from operators built without the inverse
+    mass matrices (``build_operators(..., lean=True)``) gets a zero ``minv`` for
+    ``DeviceMesh.set_geometry`` to fill on the device.
+    """
     ref = ops.ref
     if ref.kind not in KIND_IDS or not 0 <= ref.order <= MAX_ORDER:
         raise NotImplementedError(f"device kernels cover tri/quad p=0..{MAX_ORDER}, not {ref.kind} p={ref.order}")
@@ -134,11 +139,14 @@ def host_arrays(ops, *, force_general: bool = False) -> dict:
     if affine:
         out["geo"] = np.ascontiguousarray(affine_inverse_jacobian(ops).T)
     else:
-        if getattr(ops, "inv_mass", None) is None:
-            raise ValueError("general geometry needs the inverse mass matrices (build_operators(..., lean=False))")
+        lean = getattr(ops, "inv_mass", None) is None
+        if lean and not device_metrics:
+            raise ValueError("general geometry needs the inverse mass matrices (build_operators(..., lean=False)) "
+                             "or device_metrics=True")
         Xv = np.asarray(ops.node_coords)[np.asarray(topo.elem_nodes)]  # (E, NV, 2), Q = 1: the vertices
         out["geo"] = np.ascontiguousarray(np.concatenate([Xv[:, :, 0].T, Xv[:, :, 1].T], axis=0))
-        out["minv"] = np.ascontiguousarray(np.asarray(ops.inv_mass).reshape(E, -1).T)
+        out["minv"] = (np.zeros((int(ref.n_basis) ** 2, E)) if lean else
+                       np.ascontiguousarray(np.asarray(ops.inv_mass).reshape(E, -1).T))
     out["area"] = np.asarray(ops.elem_area, dtype=float)
     ed = topo.edges
     ni = ed.n_interior
@@ -193,16 +201,19 @@ def concat_arrays(parts: list[dict]) -> dict:
 class DeviceMesh:
     """Device-resident geometry and connectivity of one mesh (or one batch bucket)."""
 
-    def __init__(self, ops=None, device=None, *, force_general: bool = False, arrays: dict | None = None, ref=None):
+    def __init__(self, ops=None, device=None, *, force_general: bool = False, arrays: dict | None = None, ref=None,
+                 device_metrics: bool = False):
         import torch
 
         self.torch = torch
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise capi.NativeError("the B200 backend runs on a CUDA device only")
+        rebuild = False
         if arrays is None:
-            arrays = host_arrays(ops, force_general=force_general)
+            arrays = host_arrays(ops, force_general=force_general, device_metrics=device_metrics)
             ref = ops.ref
+            rebuild = device_metrics
         self.ref = ref
         self.kind, self.order = ref.kind, int(ref.order)
         self.np_ = int(ref.n_basis)
@@ -243,6 +254,8 @@ class DeviceMesh:
         m.lim_scale = self.lim_scale.data_ptr()
         self.c = m
         self.c_ref = C.byref(m)
+        if rebuild:  # metric terms built here from the node coordinates (nzb_geometry)
+            self.set_geometry(np.asarray(ops.node_coords, float), np.asarray(ops.topology.elem_nodes)[:, : self.nf])
 
     def set_geometry(self, X, elem_nodes) -> None:
         """Rebuild this mesh's metric terms on the device from node coordinates (``nzb_geometry``).

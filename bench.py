@@ -70,10 +70,10 @@ def microbench_state(n_elem, nbf, gamma=1.4, seed=0):
     return np.ascontiguousarray(np.stack([rho, rho * vx, rho * vy, E], -1))
 
 
-def microbench_case(nx=1000, nr=500):
-    topo, xf, rf = pkg("mesh").channel_topology("tri", nx=nx, nr=nr)
+def microbench_case(nx=1000, nr=500, kind="tri", order=3):
+    topo, xf, rf = pkg("mesh").channel_topology(kind, nx=nx, nr=nr)
     coords = pkg("mesh").rectangle_coords(xf, rf)
-    ops = pkg("operators").build_operators(topo, coords, 3, lean=True)
+    ops = pkg("operators").build_operators(topo, coords, order, lean=True)
     return ops, microbench_state(ops.n_elem, ops.ref.n_basis)
 
 
@@ -161,14 +161,15 @@ def solve_device(bk, U0_dev_soa, opts, scale, torch):
     return converged, done, res, launches
 
 
-def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
-    ops, U = microbench_case(nx, nr)
-    E = ops.n_elem
-    out = {"workload": f"residual microbench: {E} straight-sided cubic triangles (Np=10), unit rectangle {nx}x{nr} cells",
-           "l2": f"state {U.nbytes / 1e6:.0f} MB vs 126 MB L2", "kernels": {}}
+def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500, kind="tri", order=3):
+    ops, U = microbench_case(nx, nr, kind, order)
+    E, NP = ops.n_elem, int(ops.ref.n_basis)
+    shape = {"tri": "triangles", "quad": "quadrilaterals"}[kind]
+    out = {"workload": f"residual microbench: {E} straight-sided p={order} {shape} (Np={NP}), unit rectangle {nx}x{nr} "
+                       f"cells", "l2": f"state {U.nbytes / 1e6:.0f} MB vs 126 MB L2", "kernels": {}}
     results = {}
     for flux in ("roe", "hllc", "ausmup"):
-        bk = B(ops, cfg.FlowConditions(flux=flux), cfg.SolverOptions(cfl=0.5))
+        bk = B(ops, cfg.FlowConditions(flux=flux), cfg.SolverOptions(cfl=0.5), device_metrics=kind != "tri")
         bk.mesh.pack(U, bk._S[0])
         st = torch.cuda.current_stream()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -195,7 +196,7 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
                 bk.mesh.pack(U, bk._S[0])
                 torch.cuda.synchronize()
                 S0, S1, S2 = bk._S
-                factor = cfg.step_coefficient(3, 0.5, "ssprk3")
+                factor = cfg.step_coefficient(order, 0.5, "ssprk3")
                 for V, U0_, o, stage, a, b in ((S0, None, S2, 1, 0.0, 1.0), (S2, S0, S1, 2, 0.75, 0.25),
                                               (S1, S0, S0, 3, 1 / 3, 2 / 3)):
                     args = lib_capi.StageArgs()
@@ -216,11 +217,16 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
                 results[f"stage{k}_hllc"] = float(np.mean(stimes[k]))
         del bk
         torch.cuda.empty_cache()
-    # algorithmic bytes per element: state in/out, geometry, connectivity, edges once
-    S = 10 * 4 * 8
+    # algorithmic bytes per element: state in/out, geometry (affine: inverse Jacobian and
+    # det; general: vertices and the inverse mass), connectivity, edges once
+    S = NP * 4 * 8
     n_edge = ops.n_edges_total
-    base = 40 + 36 + 32.0 * n_edge / E
-    alg = {"residual": 2 * S + base + 8, "stage1": 2 * S + base + 8 + 8, "stage23": 3 * S + base + 8 + 8}
+    nf = 3 if kind == "tri" else 4
+    geo = 40 if kind == "tri" else 2 * nf * 8  # the residual applies no inverse mass
+    minv = 0 if kind == "tri" else NP * NP * 8  # general geometry: per-element inverse mass, read by rates and stages
+    base = geo + 12 * nf + 32.0 * n_edge / E
+    alg = {"residual": 2 * S + base + 8, "stage1": 2 * S + base + minv + 8 + 8,
+           "stage23": 3 * S + base + minv + 8 + 8}
     for name, t in results.items():
         b = alg["residual"] if name.startswith("residual") else (alg["stage1"] if name.startswith("stage1") else alg["stage23"])
         out["kernels"][name] = {"ms": t * 1e3, "alg_bytes_per_elem": b, "gbs": b * E / t / 1e9}
@@ -228,7 +234,8 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500):
     k = out["kernels"][dom]
     # DRAM bytes per element of each kernel from an ncu capture of 490,000 cubic triangles
     # (profiles/k_element_stage_tri_p3_490k.md), scaled to this launch by its element count
-    traffic = {"residual_roe": 1055.0, "stage1_hllc": 1135.0, "stage2_hllc": 1503.0, "stage3_hllc": 1447.0}
+    traffic = ({"residual_roe": 1055.0, "stage1_hllc": 1135.0, "stage2_hllc": 1503.0, "stage3_hllc": 1447.0}
+               if (kind, order) == ("tri", 3) else {})
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": k["gbs"], "peak": peak_gbs, "unit": "GB/s",
                        "frac": k["gbs"] / peak_gbs, "peak_source": peak_kind,
                        "traffic": traffic[dom] * E if dom in traffic else None,
@@ -700,6 +707,8 @@ def main():
     ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
     ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
     ap.add_argument("--micro-nr", type=int, default=500, help="microbench cells across")
+    ap.add_argument("--micro-kind", choices=("tri", "quad"), default="tri", help="microbench element kind (profiling)")
+    ap.add_argument("--micro-order", type=int, default=3, help="microbench order (profiling)")
     ap.add_argument("--vjp-only", action="store_true", help="run only the adjoint-kernel microbench (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -726,7 +735,7 @@ def main():
     if args.micro_only:
         peak, kind = load_peaks()
         print(json.dumps(microbench(torch, pkg("capi"), pkg("backend").B200Backend, pkg("config"), peak, kind,
-                                    args.micro_nx, args.micro_nr)))
+                                    args.micro_nx, args.micro_nr, args.micro_kind, args.micro_order)))
         return
     line = run_ours(args, rank, world, torch, dist)
     if rank == 0:

@@ -53,3 +53,17 @@ def test_residual_on_a_device_built_mesh(cuda, kind, p):
     R_ref, w_ref = ref.residual(g["U"])
     R, w = bk.residual(g["U"])
     assert rel(R, R_ref) < 1e-12 and rel(w, w_ref) < 1e-12
+
+
+def test_lean_operators_with_device_metrics(cuda):
+    """Operators built without inverse mass matrices: the device builds them, the residual is unchanged."""
+    cfg, opm = pkg("config"), pkg("operators")
+    ops, g = tiny_ops("quad", 3)
+    lean = opm.build_operators(ops.topology, ops.node_coords, 3, lean=True)
+    flow, opts = cfg.FlowConditions(flux="roe"), cfg.SolverOptions()
+    ref = pkg("backend").B200Backend(ops, flow, opts)
+    bk = pkg("backend").B200Backend(lean, flow, opts, device_metrics=True)
+    assert rel(bk.mesh.arrays["minv"].cpu().numpy(), ref.mesh.arrays["minv"].cpu().numpy()) < 1e-11
+    R_ref, _ = ref.residual(g["U"])
+    R, _ = bk.residual(g["U"])
+    assert rel(R, R_ref) < 1e-12
