@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import json
 
+import numpy as np
 import pytest
 
 from conftest import GOLDEN, pkg
@@ -78,3 +79,26 @@ def test_sampled_sweep_matches_the_reference(cuda):
     assert len(chaotic) <= 2, chaotic
     converged = sum(ref_category(rows[k]) == "converged" for k in index)
     assert converged == sum(b.converged for b in res)
+
+
+def test_sweep_table_matches_the_reference_rows(cuda):
+    """run_sweep's table on a slice of the sampled sweep: outcomes and observables per point."""
+    ref = json.load(open(f"{GOLDEN}/sweep_reference.json"))
+    sweep = pkg("sweep")
+    pts = sweep.sample_points(ref["n"], ref["seed"])[:12]
+    res = sweep.run_sweep(pts, max_iterations=ref["max_iterations"])
+    rows = {r["point"]: r for r in ref["rows"]}
+    assert res.n_points == 12
+    for k in range(12):
+        r = rows[k]
+        if r["refused"]:
+            assert res.status[k] == "refused" and not res.converged[k]
+            continue
+        assert res.converged[k] == r["converged"]
+        if r["converged"]:
+            assert res.iterations[k] == r["iterations"]
+            for key in ("thrust", "mass_flow_in", "exit_mach"):
+                assert abs(res[key][k] - r[key]) <= 1e-9 * abs(r[key]), key
+        else:
+            assert np.isnan(res["thrust"][k])
+    assert list(res["area_ratio"]) == [p.area_ratio for p in pts]
