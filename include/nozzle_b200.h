@@ -31,6 +31,11 @@
  *                                 DifferentiableCase.adjoint_solve src/sensitivity.py:289-383
  *   nzb_vjp_coords               jax.vjp of the residual w.r.t. the design variables
  *                                 through the node coordinates     src/sensitivity.py:453-458
+ *   nzb_observables              boundary_trace, axial_momentum_flux, mass_flux, entropy_error
+ *                                 and the exit averages of performance()
+ *                                                                  src/post/postprocess.py:56-255
+ *   nzb_geometry                 the coordinate-dependent part of build_operators
+ *                                                                  src/spatial/operators.py:240-303
  */
 #ifndef NOZZLE_B200_H
 #define NOZZLE_B200_H
