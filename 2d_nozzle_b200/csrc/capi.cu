@@ -84,6 +84,8 @@ static int dispatch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cud
     return fail("too many elements for one launch");
   if (m.edge_pass && w.op != OP_LIMIT && (!m.edge_conn || !m.edge_flux || !m.edge_speed))
     return fail("the edge pass needs edge_conn, edge_flux and edge_speed");
+  if (m.edge_pass && (reinterpret_cast<uintptr_t>(m.edge_flux) & 15) != 0)
+    return fail("edge_flux must be 16-byte aligned");
   if (ph.limiter == 2 && m.order > 0 && (w.op == OP_STAGE || w.op == OP_LIMIT)) {
     if (m.elem_inst) return fail("the Superbee limiter applies to a mesh of one instance");
     if (!m.elem_share || !m.lim_means || !m.lim_scale)

@@ -369,7 +369,8 @@ __device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
 // The edge pass: one thread per edge evaluates the numerical flux at the
 // edge's points, once -- the owner's trace (phi_face[0, f]) as the left state,
 // the neighbour's (phi_face[1, nf]) as the right, the owner's normal -- and
-// stores w_q |dX/dsigma| Fhat (edge_flux, (NQF, 4, n_edge)) and max_q s_q
+// stores w_q |dX/dsigma| Fhat (edge_flux, (n_edge, NQF, 4): an edge's values
+// contiguous, read as whole 32-byte sectors by both its elements) and max_q s_q
 // (edge_speed), the reference's edge_pass (src/backends/_numba_kernels.py:
 // 484-583).  The element kernel with EP = true lifts them.  The arithmetic is
 // the fused kernel's, so both variants give bit-identical residuals.
@@ -431,8 +432,9 @@ __global__ void __launch_bounds__(128) k_edge(const nzb_mesh m, const nzb_physic
     }
     smax = sp > smax ? sp : smax;
     const double scale = jac * c_tab[S::O_WF + q];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) m.edge_flux[(int64_t)(q * 4 + s) * NK + k] = F[s] * scale;
+    double2* dst = reinterpret_cast<double2*>(m.edge_flux + ((int64_t)k * NQF + q) * 4);
+    dst[0] = make_double2(F[0] * scale, F[1] * scale);
+    dst[1] = make_double2(F[2] * scale, F[3] * scale);
   }
   m.edge_speed[k] = smax;
 }
@@ -502,7 +504,6 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
     if constexpr (EP) {
       // the edge pass (k_edge) has left w |dX/dsigma| Fhat at every edge point
       // and max_q s_q per edge; lift them with this element's side of the face
-      const int64_t NK = m.n_edge;
 #pragma unroll 1
       for (int f = 0; f < NF; ++f) {
         const int code = __ldg(m.face_code + f * E + e);
@@ -512,9 +513,9 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
         const double coef = (side ? -1.0 : 1.0) * fs;
 #pragma unroll 1
         for (int q = 0; q < NQF; ++q) {
-          double fwc[4];
-#pragma unroll
-          for (int s = 0; s < 4; ++s) fwc[s] = __ldg(m.edge_flux + (int64_t)(q * 4 + s) * NK + k) * coef;
+          const double2* src = reinterpret_cast<const double2*>(m.edge_flux + ((int64_t)k * NQF + q) * 4);
+          const double2 f01 = __ldg(src), f23 = __ldg(src + 1);
+          const double fwc[4] = {f01.x * coef, f01.y * coef, f23.x * coef, f23.y * coef};
 #pragma unroll
           for (int j = 0; j < NE; ++j) {
             const double cj = pfe<K, P>(side, f, j, q);

@@ -103,7 +103,7 @@ typedef struct {
   const double* inst_p_back;
   const int32_t* edge_conn; /* (3, n_edge): owner element, neighbour (-1: boundary),
                                owner face | neighbour face << 3 | boundary tag << 6 */
-  double* edge_flux;        /* (NQF, 4, n_edge) scratch of the edge pass */
+  double* edge_flux;        /* (n_edge, NQF, 4) scratch of the edge pass, 16-byte aligned */
   double* edge_speed;       /* (n_edge) scratch of the edge pass */
   const double* elem_share; /* (E) A_e / A_domain, for the Superbee limiter (limiter 2) */
   double* lim_means;        /* (4, E) scratch of the Superbee limiter */
