@@ -173,6 +173,19 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, NZB_MINB_VJP * 128 / Launch<
       const double nx = __ldg(m.edge_geo + 4 * (int64_t)k + 0);
       const double ny = __ldg(m.edge_geo + 4 * (int64_t)k + 1);
       const double jac = __ldg(m.edge_geo + 4 * (int64_t)k + 2);
+      // the neighbour's edge coefficients (scattered reads), once per face
+      double un[NE][4], lnb[NE][4];
+      if (nb >= 0) {
+#pragma unroll
+        for (int j = 0; j < NE; ++j) {
+          const int n = edge_node(K, P, nf, j);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            un[j][s] = __ldg(U + (s * NP + n) * E + nb);
+            lnb[j][s] = __ldg(L + (s * NP + n) * E + nb);
+          }
+        }
+      }
 #pragma unroll 1
       for (int q = 0; q < NQF; ++q) {
         double tc[4] = {0.0, 0.0, 0.0, 0.0}, lc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -191,11 +204,10 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, NZB_MINB_VJP * 128 / Launch<
 #pragma unroll
           for (int j = 0; j < NE; ++j) {
             const double c = pfe<K, P>(1 - side, nf, j, q);
-            const int n = edge_node(K, P, nf, j);
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-              tn[s] = fma(c, __ldg(U + (s * NP + n) * E + nb), tn[s]);
-              ln[s] = fma(c, __ldg(L + (s * NP + n) * E + nb), ln[s]);
+              tn[s] = fma(c, un[j][s], tn[s]);
+              ln[s] = fma(c, lnb[j][s], ln[s]);
             }
           }
         }
