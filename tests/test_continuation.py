@@ -47,3 +47,42 @@ def test_mesh_mismatch_raises():
     b = nz.build_case(contour="smooth", element="tri", order=2, refine=1)
     with pytest.raises(ValueError, match="same mesh"):
         co.change_order(a.initial_state(), a.operators, b.operators)
+
+
+class _FakeBatch:
+    """Stands in for BatchSolver on the host: records each batch, 'converges' every instance at once."""
+
+    made: list = []
+
+    def __init__(self, instances, device=None):
+        self.instances = instances
+        _FakeBatch.made.append([(i.ops.ref.order, i.flow.flux, i.opts.tolerance) for i in instances])
+
+    def run(self):
+        return 1
+
+    def results(self, with_state=True):
+        from types import SimpleNamespace
+
+        return [SimpleNamespace(U=i.U0, converged=True, iterations=10 * (i.ops.ref.order + 1), residual=0.0,
+                                status="converged") for i in self.instances]
+
+
+def test_batched_stages_group_by_flux_and_sum_iterations(monkeypatch):
+    nz, cfg, co = pkg("nozzle"), pkg("config"), pkg("continuation")
+    monkeypatch.setattr(pkg("batch"), "BatchSolver", _FakeBatch)
+    _FakeBatch.made = []
+    on = cfg.SolverOptions(p_continuation=True, tolerance=1e-9)
+    cases = [nz.build_case(element="tri", order=2, refine=0, contour="smooth", options=on,
+                           flow=cfg.FlowConditions(flux=f)) for f in ("roe", "hllc")]
+    cases.append(nz.build_case(element="quad", order=1, refine=0, contour="smooth", options=on,
+                               flow=cfg.FlowConditions(flux="hllc")))
+    warm = [None, None, cases[2].initial_state()]  # the third starts warm: its target order only
+    got = co.solve_batch(cases, warm_starts=warm)
+    assert [r.orders for r in got] == [[0, 1, 2], [0, 1, 2], [1]]
+    assert [r.iterations for r in got] == [10 + 20 + 30, 10 + 20 + 30, 20]
+    # stage 0: roe alone, then hllc (tri p0) with the warm quad (target order, its own tolerance)
+    assert _FakeBatch.made[0] == [(0, "roe", 1e-4)]
+    assert _FakeBatch.made[1] == [(0, "hllc", 1e-4), (1, "hllc", 1e-9)]
+    assert _FakeBatch.made[-1] == [(2, "hllc", 1e-9)]
+    assert all(r.converged for r in got) and got[0].operators.ref.order == 2
