@@ -348,6 +348,13 @@ __device__ __forceinline__ void prefetch_line(const double* p) { asm volatile("p
 #ifndef NZB_MINB_STAGE
 #define NZB_MINB_STAGE 1
 #endif
+// Resident 128-thread blocks per SM asked of the compiler for the edge pass:
+// 4 caps it at 128 registers (from 168, with a few spills), 16 warps per SM
+// instead of 12 -- measured 14 % faster on 1 M linear triangles.
+#ifndef NZB_MINB_EDGE
+#define NZB_MINB_EDGE 4
+#endif
+
 template <int K, int P>
 struct Launch {
   static constexpr int NP = Shape<K, P>::NP;
@@ -375,7 +382,7 @@ __device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
 // 484-583).  The element kernel with EP = true lifts them.  The arithmetic is
 // the fused kernel's, so both variants give bit-identical residuals.
 template <int K, int P>
-__global__ void __launch_bounds__(128) k_edge(const nzb_mesh m, const nzb_physics ph, const double* __restrict__ V) {
+__global__ void __launch_bounds__(128, NZB_MINB_EDGE) k_edge(const nzb_mesh m, const nzb_physics ph, const double* __restrict__ V) {
   using S = Shape<K, P>;
   constexpr int NP = S::NP, NQF = S::NQF, NE = S::NE;
   const int64_t NK = m.n_edge, E = m.n_elem;
