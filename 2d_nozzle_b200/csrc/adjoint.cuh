@@ -101,12 +101,18 @@ __device__ __forceinline__ bool euler_flux_vjp(const double (&U)[4], double g, c
 
 // Resident blocks per SM asked of the compiler for k_vjp (as NZB_MINB_* for
 // the forward kernels): registers per thread are capped at 65536 / (MINB * NT).
+// Linear elements run with three blocks (170 registers): measured 13-20 %
+// faster on the design sweep's p = 1 buckets; higher orders spill and slow down.
 #ifndef NZB_MINB_VJP
 #define NZB_MINB_VJP 1
 #endif
+template <int K, int P>
+struct VjpBounds {
+  static constexpr int MINB = (P <= 1 ? 3 : NZB_MINB_VJP) * 128 / Launch<K, P>::NT;
+};
 
 template <int K, int P, bool AFF>
-__global__ void __launch_bounds__(Launch<K, P>::NT, NZB_MINB_VJP * 128 / Launch<K, P>::NT)
+__global__ void __launch_bounds__(Launch<K, P>::NT, VjpBounds<K, P>::MINB)
     k_vjp(const nzb_mesh m, const nzb_physics ph, const AdjWork w) {
   using S = Shape<K, P>;
   using D4 = Dual<4>;
