@@ -82,3 +82,35 @@ def test_physics_struct_constants():
     assert list(ph.norm_w) == pytest.approx([1.0, 1 / 0.7483314773547883, 1 / 0.7483314773547883, 1 / 0.56])
     with pytest.raises(NotImplementedError):
         layout.physics_struct(types.SimpleNamespace(flux="slau2"), cfg.SolverOptions(), None)
+
+
+def test_device_metric_arrays_from_lean_operators():
+    """Lean operators (no inverse mass) give general-geometry arrays with a zero minv to fill on the device."""
+    lay, opm = pkg("layout"), pkg("operators")
+    from conftest import tiny_ops
+
+    ops, _ = tiny_ops("quad", 2)
+    lean = opm.build_operators(ops.topology, ops.node_coords, 2, lean=True)
+    with pytest.raises(ValueError, match="inverse mass"):
+        lay.host_arrays(lean)
+    full, dev = lay.host_arrays(ops), lay.host_arrays(lean, device_metrics=True)
+    assert dev["minv"].shape == full["minv"].shape and not dev["minv"].any()
+    for k in ("geo", "area", "face_nbr", "face_code", "face_edge", "edge_geo", "edge_conn"):
+        assert np.array_equal(dev[k], full[k]), k
+
+
+def test_face_tangent_table_gives_the_edge_jacobians():
+    """|sum_v T[f, v] X_v| is each face's |dX/dsigma| (straight faces), for both element kinds."""
+    lay = pkg("layout")
+    from conftest import tiny_ops
+
+    for kind, p in (("tri", 1), ("quad", 1)):
+        ops, _ = tiny_ops(kind, p)
+        T = lay.face_tangent_table(ops.ref)
+        nv = 3 if kind == "tri" else 4
+        Xe = np.asarray(ops.node_coords)[np.asarray(ops.topology.elem_nodes)[:, :nv]]
+        ed = ops.topology.edges
+        own_e = np.concatenate([ed.iedge_elem[:, 0], ed.bedge_elem])
+        own_f = np.concatenate([ed.iedge_face[:, 0], ed.bedge_face])
+        t = np.einsum("kv,kvd->kd", T[own_f, :nv], Xe[own_e])
+        assert np.allclose(np.hypot(t[:, 0], t[:, 1]), np.asarray(ops.edge_jac)[:, 0], rtol=1e-14, atol=0)
