@@ -121,7 +121,8 @@ def optimise_case(case, starts, names, bounds, *, objective="thrust", maximise=T
 
     ``starts``: points (one value per name in ``names``); each evaluation is the
     objective and its adjoint gradient with respect to ``names``.  A member
-    whose forward solve fails evaluates to NaN, which ends its L-BFGS-B run.
+    whose forward solve fails evaluates to NaN, which L-BFGS-B reports as a
+    failed run (its result's ``success`` is false or its value not finite).
     """
     from .adjoint import BatchGradient
 

@@ -57,3 +57,34 @@ def test_a_failed_evaluation_ends_every_run():
 
     with pytest.raises(FloatingPointError, match="planted"):
         opt.minimize_batch(evaluate, [np.zeros(3), np.ones(3)], BOUNDS)
+
+
+def test_optimise_case_batches_members_and_maps_failures(monkeypatch):
+    """optimise_case turns each round into one BatchGradient; a failed member evaluates to NaN."""
+    from types import SimpleNamespace
+
+    ad, opt = pkg("adjoint"), pkg("optimise")
+    seen = []
+
+    class FakeBatch:
+        def __init__(self, case, members, objective, names):
+            self.members, self.names = members, names
+            seen.append(len(members))
+
+        def run(self, adjoint_tolerance=1e-8):
+            out = []
+            for m in self.members:
+                x = np.array([m[k] for k in self.names])
+                if x[0] > 1.9:  # a member whose forward solve fails
+                    out.append(SimpleNamespace(value=float("nan"), grad=None))
+                else:
+                    out.append(SimpleNamespace(value=float(-(x - 0.5) @ (x - 0.5)),
+                                               grad={k: float(-2.0 * (v - 0.5)) for k, v in zip(self.names, x)}))
+            return out
+
+    monkeypatch.setattr(ad, "BatchGradient", FakeBatch)
+    got = opt.optimise_case(None, [np.array([0.0, 1.0]), np.array([1.95, 0.0])], ("a", "b"),
+                            [(-2.0, 2.0), (-2.0, 2.0)], maxiter=20)
+    assert seen[0] == 2 and sum(seen) == len(got[0].history) + len(got[1].history)
+    assert np.allclose(got[0].x, [0.5, 0.5], atol=1e-5) and got[0].value == pytest.approx(0.0, abs=1e-9)
+    assert not np.isfinite(got[1].history[0][1]) and not (got[1].success and np.isfinite(got[1].value))
