@@ -44,6 +44,8 @@ class Mesh(C.Structure):
         ("elem_share", P),
         ("lim_means", P),
         ("lim_scale", P),
+        ("split", I32),
+        ("reserved_split", I32),
     ]
 
 

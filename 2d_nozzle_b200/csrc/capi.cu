@@ -17,6 +17,7 @@
 #include "adjoint_dispatch.cuh"
 #include "element.cuh"
 #include "forward_dispatch.cuh"
+#include "split.cuh"
 #include "nozzle_b200.h"
 
 namespace nzb {
@@ -51,6 +52,7 @@ static int check_mesh(const nzb_mesh* m) {
   if (m->order < 0 || m->order > MAX_ORDER) return fail("order must lie in 0..3");
   if (m->affine && m->kind != NZB_TRI) return fail("affine geometry is for straight-sided triangles");
   if (m->n_elem <= 0) return fail("mesh has no elements");
+  if (m->split != 0 && m->split != 1 && m->split != SPLIT_T) return fail("split must be 0, 1 or 4 threads per element");
   if (!m->area || !m->face_nbr || !m->face_code || !m->face_edge || !m->edge_geo)
     return fail("mesh arrays area/face_nbr/face_code/face_edge/edge_geo are required");
   if (!m->geo || (!m->affine && !m->minv))
@@ -73,7 +75,14 @@ static int block_threads(int kind, int order) {
   }
   return 128;
 }
+// Blocks of the forward element kernel (= norm partial slots of stage 1):
+// 32 elements per block with four threads per element.
 static int64_t element_blocks(const nzb_mesh& m) {
+  const int bt = (m.split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
+  return (m.n_elem + bt - 1) / bt;
+}
+// Blocks of the adjoint element kernels (one thread per element).
+static int64_t adjoint_blocks(const nzb_mesh& m) {
   const int bt = block_threads(m.kind, m.order);
   return (m.n_elem + bt - 1) / bt;
 }
@@ -425,7 +434,7 @@ static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
 // ---- adjoint ------------------------------------------------------------------
 // The adjoint kernels live in adjoint_tri.cu / adjoint_quad.cu.
 static int dispatch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
-  if (element_blocks(m) > 0x7fffffff) return fail("too many elements for one launch");
+  if (adjoint_blocks(m) > 0x7fffffff) return fail("too many elements for one launch");
   const cudaError_t e = m.kind == NZB_TRI ? vjp_launch_tri(m, ph, w, st) : vjp_launch_quad(m, ph, w, st);
   return cuda_check(e, "vjp kernel launch");
 }
@@ -641,7 +650,8 @@ int nzb_upload_tables(int kind, int order, const double* tables, int64_t n) {
       cuda_check(upload_tables_fwd_tri(tables, (size_t)n, off), "table upload (triangles)") ||
       cuda_check(upload_tables_fwd_quad(tables, (size_t)n, off), "table upload (quadrilaterals)") ||
       cuda_check(upload_tables_tri(tables, (size_t)n, off), "table upload (adjoint, triangles)") ||
-      cuda_check(upload_tables_quad(tables, (size_t)n, off), "table upload (adjoint, quadrilaterals)"))
+      cuda_check(upload_tables_quad(tables, (size_t)n, off), "table upload (adjoint, quadrilaterals)") ||
+      cuda_check(kind == NZB_TRI ? prepare_split_tri(order) : prepare_split_quad(order), "split kernel attributes"))
     return -1;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -759,7 +769,7 @@ int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_arg
   return dispatch(*mesh, *phys, w, (cudaStream_t)stream);
 }
 
-int64_t nzb_norm_blocks(int64_t n_elem) { return n_elem <= 0 ? 0 : (n_elem + 63) / 64; }
+int64_t nzb_norm_blocks(int64_t n_elem) { return n_elem <= 0 ? 0 : (n_elem + SPLIT_EB - 1) / SPLIT_EB; }
 
 int64_t nzb_element_blocks(const nzb_mesh* mesh) { return mesh ? element_blocks(*mesh) : -1; }
 

@@ -24,6 +24,9 @@ NZB_INTERNAL cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_ph
                                                  cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
+// raise the split kernels' dynamic shared-memory limit for one order (current device)
+NZB_INTERNAL cudaError_t prepare_split_tri(int order);
+NZB_INTERNAL cudaError_t prepare_split_quad(int order);
 NZB_INTERNAL cudaError_t upload_tables_fwd_tri(const double* src, size_t count, size_t offset);
 NZB_INTERNAL cudaError_t upload_tables_fwd_quad(const double* src, size_t count, size_t offset);
 

@@ -1,0 +1,757 @@
+// split.cuh -- the element kernel with four threads per element.
+//
+// A block of four warps owns 32 elements, one per lane; the warp index r is
+// the part of the element's work that thread does.  Every table operand stays
+// a compile-time constant-bank address (or, for the face basis, a shared-memory
+// read): a warp's 32 lanes always want the same table entry, because they do
+// the same part of the work for 32 different elements.  The phases, separated
+// by block barriers:
+//
+//   0  the block's states are staged in shared memory (coalesced plane loads:
+//      component s, node i, 32 consecutive elements), with the face basis;
+//   A1 warp r < NF evaluates face r's numerical fluxes at its points -- the
+//      owner's trace as the left state, the owner's normal, in one rolled loop
+//      (one copy of the flux code in the kernel, so both elements of an edge
+//      compute bit-identical fluxes); a warp without a face (triangles) takes
+//      the last volume points meanwhile;
+//   A2 the other volume points (interpolation, Euler flux, contravariant
+//      flux), a compile-time share per warp;
+//   B  warp r projects component s = r: the face lifts, then the weak-form
+//      volume sums of every node from the fluxes of all points; then the
+//      inverse mass (affine: the reference table, by component; general:
+//      the element's own matrix, by rows), the stage update and the local step;
+//   C  the positivity limiter: every warp forms the element's cell average,
+//      repair and Lebesgue screen (identical arithmetic in the four warps), the
+//      probe scan is split over the warps (each a compile-time share of the
+//      probe points) and its minima and t* reduced through shared memory; the
+//      bisection replay on t* is scalar, and its rare pointwise re-checks are
+//      split over the warps too.
+//
+// The mathematics is the fused kernel's (element.cuh; src/spatial/assembly.py:
+// 52-162, src/spatial/limiter.py:103-243, src/backends/_numba_kernels.py:
+// 484-850): the same formulas with the same operands; only the association of
+// a few sums differs (face lifts per face, probe values summed by node), a
+// round-off difference.
+#pragma once
+#include <type_traits>
+
+#include "element.cuh"
+
+namespace nzb {
+
+constexpr int SPLIT_T = 4;   // threads (warps) per element
+constexpr int SPLIT_EB = 32; // elements per block, one per lane
+
+struct SplitRanges {
+  int first[SPLIT_T];
+  int count[SPLIT_T];
+};
+
+// Index of node i on edge f of the element (0..p), or -1.
+__host__ __device__ constexpr int edge_pos(int kind, int p, int f, int i) {
+  for (int j = 0; j <= p; ++j)
+    if (edge_node(kind, p, f, j) == i) return j;
+  return -1;
+}
+
+template <int K, int P>
+struct SplitPlan {
+  using S = Shape<K, P>;
+  // Costs in instruction units: a volume point (interpolation, Euler flux,
+  // contravariant flux, stores; the vertex Jacobian for general geometry) and
+  // a face (two traces, the flux and the lift at each face point).
+  static constexpr int VCOST = 4 * S::NP + 40 + (K == 1 ? 16 : 0);
+  static constexpr int FCOST = S::NQF * (12 * S::NE + 150);
+
+  // Phase A1: a warp without a face (triangles: warp 3) evaluates the last
+  // LATE volume points while the others evaluate their faces' fluxes; their
+  // FV slots must lie beyond the NF * NE * 4 slots that stage the neighbours'
+  // edge coefficients.  The rest go to phase A2, evenly.
+  static constexpr int late() {
+    if (S::NF >= SPLIT_T) return 0;
+    const int first_free = (S::NF * S::NE * 4 + 7) / 8;  // first point whose FV slots are free
+    int n = FCOST / VCOST;
+    if (n > S::NQV - first_free) n = S::NQV - first_free;
+    return n < 0 ? 0 : n;
+  }
+  static constexpr int LATE = late();
+
+  // An even split of n items over the warps.
+  static constexpr SplitRanges even(int n) {
+    SplitRanges R{};
+    int f = 0;
+    for (int r = 0; r < SPLIT_T; ++r) {
+      R.count[r] = n / SPLIT_T + (r < n % SPLIT_T ? 1 : 0);
+      R.first[r] = f;
+      f += R.count[r];
+    }
+    return R;
+  }
+};
+
+// Shared-memory layout (doubles).  Per-element arrays are [slot][32 lanes].
+template <int K, int P>
+struct SplitSmem {
+  using S = Shape<K, P>;
+  static constexpr int U = 0;                                   // [NP*4]   state, slot i*4+s
+  static constexpr int FV = U + S::NP * 4 * SPLIT_EB;           // [NQV*8]  fx_s, fe_s per point
+  static constexpr int LIFT = FV + S::NQV * 8 * SPLIT_EB;       // [NF*NQF*4] w |dX/dsigma| Fhat at face points
+  static constexpr int WAVE = LIFT + S::NF * S::NQF * 4 * SPLIT_EB;  // [NF]  s_max * length per face
+  static constexpr int PFE = WAVE + S::NF * SPLIT_EB;           // face basis table [2][NF][NE][NQF]
+  static constexpr int TOTAL = PFE + 2 * S::NF * S::NE * S::NQF;
+  static constexpr int BYTES = TOTAL * 8;
+  // after phase B: stage-1 norm partials ([4 warps][32]) and the limiter's
+  // partial minima ([4 warps][3][32]) in LIFT, the probe chunks' quadratic
+  // coefficients in FV ([4 warps][2 * 4][32])
+  static constexpr int NRM = LIFT;
+  static constexpr int RED = LIFT + SPLIT_T * SPLIT_EB;
+  static constexpr int SCR = FV;
+  // resident blocks per SM the shared memory allows (228 KB, 1 KB reserved per block), at most 4
+  static constexpr int BLOCKS = (228 * 1024) / (BYTES + 1024) < 4 ? (228 * 1024) / (BYTES + 1024) : 4;
+  static constexpr int MINB = BLOCKS < 1 ? 1 : BLOCKS;
+  // phase A1 stages the neighbours' edge coefficients in FV
+  static_assert(S::NF * S::NE * 4 <= S::NQV * 8, "FV too small to stage the neighbour coefficients");
+  static_assert(SPLIT_T * 4 <= S::NF * S::NQF * 4, "LIFT too small for the limiter partials");
+  static_assert(SPLIT_T * 8 <= S::NQV * 8, "FV too small for the probe chunks");
+  static_assert(S::NP * 4 <= S::NQV * 8, "FV too small for the projection sums of general geometry");
+};
+
+// Calls fn(integral_constant<int, r>) for the runtime warp index r (uniform
+// across a warp), so each warp runs code compiled for its own share.
+template <class F>
+__device__ __forceinline__ void for_part(int r, F&& fn) {
+  switch (r) {
+    case 0: fn(std::integral_constant<int, 0>{}); break;
+    case 1: fn(std::integral_constant<int, 1>{}); break;
+    case 2: fn(std::integral_constant<int, 2>{}); break;
+    default: fn(std::integral_constant<int, 3>{}); break;
+  }
+}
+
+// Phase A, volume share: points [Q0, Q0 + NQ) of this lane's element, in
+// chunks of at most 4 (the interpolation runs node-major, so a chunk holds
+// 16 accumulators and reads each coefficient from shared memory once).
+// The element's geometry is loaded here (L1 hits after the first warp) rather
+// than kept live across the face phase.
+template <int K, int P, bool AFF, int Q0, int NQ>
+__device__ __forceinline__ void split_volume(const double* col, double* fv, const nzb_mesh& m, int64_t e, bool active,
+                                             bool rate, double g) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NF = S::NF;
+  constexpr int CH = 4;
+  const int64_t E = m.n_elem;
+  double xx = 0, xy = 0, yx = 0, yy = 0, det = 1.0;
+  double xv[NF], yv[NF];
+#pragma unroll
+  for (int v = 0; v < NF; ++v) xv[v] = yv[v] = 0.0;
+  if (active) {
+    if (AFF) {
+      xx = __ldg(m.geo + 0 * E + e);
+      xy = __ldg(m.geo + 1 * E + e);
+      yx = __ldg(m.geo + 2 * E + e);
+      yy = __ldg(m.geo + 3 * E + e);
+      det = __ldg(m.geo + 4 * E + e);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NF; ++v) {
+        xv[v] = __ldg(m.geo + v * E + e);
+        yv[v] = __ldg(m.geo + (NF + v) * E + e);
+      }
+    }
+  }
+  // affine: (xi_x F + xi_y G) det, det only for the residual (the rate
+  // divides it out again); general: det (xi_x, xi_y) = (y_eta, -x_eta)
+  const double vs = AFF ? (rate ? 1.0 : -det) : -1.0;
+#pragma unroll
+  for (int c0 = 0; c0 < NQ; c0 += CH) {
+    const int nq = NQ - c0 < CH ? NQ - c0 : CH;
+    double uq[CH][4];
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) uq[k][s] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double ui[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) ui[s] = col[(i * 4 + s) * SPLIT_EB];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        if (k < nq) {
+          const double phi = tab<K, P>(S::O_PHI + i * NQV + Q0 + c0 + k);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) uq[k][s] = fma(phi, ui[s], uq[k][s]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+      if (k < nq) {
+        const int q = Q0 + c0 + k;
+        const Prim pr = primitives_fast(uq[k], g);
+        const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
+        const double G[4] = {pr.rho * pr.vy, pr.rho * pr.vx * pr.vy, pr.rho * pr.vy * pr.vy + pr.p, pr.rho * pr.vy * pr.H};
+        double a00 = xx, a01 = xy, a10 = yx, a11 = yy;
+        if (!AFF) {
+          double x_xi, x_eta, y_xi, y_eta;
+          point_det<K, P>(xv, yv, q, x_xi, x_eta, y_xi, y_eta);
+          a00 = y_eta;
+          a01 = -x_eta;
+          a10 = -y_xi;
+          a11 = x_xi;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          fv[(q * 8 + s) * SPLIT_EB] = (a00 * F[s] + a01 * G[s]) * vs;
+          fv[(q * 8 + 4 + s) * SPLIT_EB] = (a10 * F[s] + a11 * G[s]) * vs;
+        }
+      }
+    }
+  }
+}
+
+// Phase C, probe share: probe points [P0, P0 + NPR) of the reference's probe
+// set (volume points, then the element's own face points with the basis of
+// its side of each face, src/spatial/limiter.py:78-95), node-major from the
+// shared-memory state; the raw minima and t* over them (see probe_scan).
+//
+// The quadratic's coefficients of a chunk's points go to this warp's slots
+// of shared memory (scr, stride 32) and the roots are taken in a rolled loop:
+// unrolled over the points, the square roots and divisions would hold more
+// registers than the kernel has.
+template <int K, int P, int P0, int NPR>
+__device__ __forceinline__ void split_probe(const double* col, double* scr, const double (&ub)[4], int sides,
+                                            double eps_p, double g, double& rmin, double& pmin, double& tstar) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF;
+  const double e1 = eps_p / (g - 1.0);
+  const double c = ub[3] * ub[0] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) - e1 * ub[0];
+  constexpr int CH = 4;
+#pragma unroll
+  for (int c0 = 0; c0 < NPR; c0 += CH) {
+    // keep the next chunk's shared-memory reads from being hoisted into this one
+    asm volatile("" ::: "memory");
+    const int npr = NPR - c0 < CH ? NPR - c0 : CH;
+    double w[CH][4];
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w[k][s] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double ui[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) ui[s] = col[(i * 4 + s) * SPLIT_EB];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        if (k < npr) {
+          const int pt = P0 + c0 + k;
+          double cf;
+          if (pt < NQV) {
+            cf = tab<K, P>(S::O_PHI + i * NQV + pt);
+          } else {
+            const int f = (pt - NQV) / NQF, q = (pt - NQV) - f * NQF;
+            const int j = edge_pos(K, P, f, i);
+            if (j < 0) continue;
+            const double c0v = pfe<K, P>(0, f, j, q), c1v = pfe<K, P>(1, f, j, q);
+            cf = ((sides >> f) & 1) ? c1v : c0v;
+          }
+#pragma unroll
+          for (int s = 0; s < 4; ++s) w[k][s] = fma(cf, ui[s], w[k][s]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+      if (k < npr) {
+        rmin = w[k][0] < rmin ? w[k][0] : rmin;
+        const double pp = pressure_at(w[k], g);
+        pmin = pp < pmin ? pp : pmin;
+        const double d0 = w[k][0] - ub[0], d1 = w[k][1] - ub[1], d2 = w[k][2] - ub[2], d3 = w[k][3] - ub[3];
+        scr[(2 * k) * SPLIT_EB] = d3 * d0 - 0.5 * (d1 * d1 + d2 * d2);
+        scr[(2 * k + 1) * SPLIT_EB] = ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0;
+      }
+    }
+#pragma unroll 1
+    for (int k = 0; k < npr; ++k) {
+      const double a = scr[(2 * k) * SPLIT_EB], b = scr[(2 * k + 1) * SPLIT_EB];
+      // h stays positive for t > 0 when it starts increasing and curves up
+      if (a >= 0.0 && b >= 0.0) continue;
+      const double disc = b * b - 4.0 * a * c;
+      if (disc < 0.0) continue;
+      const double qq = -0.5 * (b + copysign(sqrt(disc), b));
+      const double r1 = a != 0.0 ? qq / a : 1e300, r2 = qq != 0.0 ? c / qq : 1e300;
+      const double p1 = r1 > 0.0 ? r1 : 1e300, p2 = r2 > 0.0 ? r2 : 1e300;
+      const double t = p1 < p2 ? p1 : p2;
+      tstar = t < tstar ? t : tstar;
+    }
+  }
+}
+
+// The pointwise minimum pressure of ubar + t (u - ubar) over probe points
+// r, r + 4, ... (the rare re-check near t*), with the fused kernel's point
+// arithmetic (probe_point): rolled, warp-uniform point index.
+template <int K, int P>
+__device__ __forceinline__ double split_pmin(const double* col, const double* s_pfe, int r, const double (&ub)[4],
+                                             double t, int sides, double g) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
+  double pmin = 1e300;
+#pragma unroll 1
+  for (int pt = r; pt < S::NPROBE; pt += SPLIT_T) {
+    double w[4] = {0.0, 0.0, 0.0, 0.0};
+    if (pt < NQV) {
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const double phi = c_tab[S::O_PHI + i * NQV + pt];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) w[s] = fma(phi, col[(i * 4 + s) * SPLIT_EB], w[s]);
+      }
+    } else {
+      const int f = (pt - NQV) / NQF, q = (pt - NQV) - f * NQF;
+      const int side = (sides >> f) & 1;
+#pragma unroll
+      for (int j = 0; j < NE; ++j) {
+        const double l = s_pfe[((side * NF + f) * NE + j) * NQF + q];
+        const int n = edge_node(K, P, f, j);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) w[s] = fma(l, col[(n * 4 + s) * SPLIT_EB], w[s]);
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) w[s] = ub[s] + t * (w[s] - ub[s]);
+    const double pp = pressure_at(w, g);
+    pmin = pp < pmin ? pp : pmin;
+  }
+  return pmin;
+}
+
+template <int K, int P, bool AFF, bool LIM>
+__global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
+    k_split(const nzb_mesh m, const nzb_physics ph, const Work w) {
+  using S = Shape<K, P>;
+  using L = SplitSmem<K, P>;
+  using PL = SplitPlan<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NF = S::NF, NE = S::NE;
+  constexpr int EB = SPLIT_EB;
+  extern __shared__ double smem[];
+  const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const int64_t E = m.n_elem;
+  const int64_t e = (int64_t)blockIdx.x * EB + lane;
+  int inst = -1;
+  if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
+  const bool active = e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0);
+  const double g = ph.gamma;
+  double* const col = smem + L::U + lane;  // this lane's state column, stride 32
+  double* const s_pfe = smem + L::PFE;
+  const bool limit_only = LIM && w.op == OP_LIMIT;
+  const bool stage = LIM && w.op == OP_STAGE;
+  const bool rate = w.op != OP_RESIDUAL;
+
+  // ---- phase 0: face basis and states into shared memory
+  for (int k = threadIdx.x; k < 2 * NF * NE * NQF; k += SPLIT_T * 32) s_pfe[k] = c_tab[S::O_PFE + k];
+#pragma unroll
+  for (int c = r; c < NP * 4; c += SPLIT_T) {
+    const int i = c >> 2, s = c & 3;
+    col[c * EB] = active ? __ldg(w.V + ((int64_t)s * NP + i) * E + e) : 0.0;
+  }
+  __syncthreads();
+
+  int sides = 0;
+  if (active) sides = face_sides<K, P>(m, e);
+  double nrm = 0.0;
+
+  if (!limit_only) {
+    // ---- phase A1: face r's fluxes (one rolled copy of the flux code), or,
+    // for a warp without a face, the last volume points (their slots lie
+    // beyond the neighbour coefficients staged at the start of FV)
+    if (r < NF) {
+      const int f = r;
+      double smax = 0.0, len = 0.0;
+      double* fw = smem + L::LIFT + f * NQF * 4 * EB + lane;  // (q, s) fluxes of face f
+      if (active) {
+        const int code = __ldg(m.face_code + f * E + e);
+        const int k = __ldg(m.face_edge + f * E + e);
+        const int nb = __ldg(m.face_nbr + f * E + e);
+        const int side = code & 1;
+        const int nf = (code >> 1) & 7;
+        const int tag = code >> 4;
+        const double nx = __ldg(m.edge_geo + 4 * (int64_t)k + 0);
+        const double ny = __ldg(m.edge_geo + 4 * (int64_t)k + 1);
+        const double jac = __ldg(m.edge_geo + 4 * (int64_t)k + 2);
+        len = __ldg(m.edge_geo + 4 * (int64_t)k + 3);
+        // affine rate: the face term carries -1/det (the rate is -M^-1 R with M = det M_ref)
+        const double fs = (AFF && rate) ? -1.0 / __ldg(m.geo + 4 * E + e) : 1.0;
+        // the neighbour's edge coefficients, staged in this face's FV slots
+        double* nbc = smem + L::FV + f * NE * 4 * EB + lane;
+        if (nb >= 0) {
+#pragma unroll
+          for (int j = 0; j < NE; ++j) {
+            const int n = edge_node(K, P, nf, j);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) nbc[(j * 4 + s) * EB] = __ldg(w.V + ((int64_t)s * NP + n) * E + nb);
+          }
+        }
+        int own_node[NE];
+#pragma unroll
+        for (int j = 0; j < NE; ++j) own_node[j] = edge_node(K, P, f, j);
+        const double coef = (side ? -1.0 : 1.0) * fs;
+        const double* own = s_pfe + (side * NF + f) * NE * NQF;
+        const double* oth = s_pfe + ((1 - side) * NF + nf) * NE * NQF;
+#pragma unroll 1
+        for (int q = 0; q < NQF; ++q) {
+          // canonical (owner's) point q: own trace with phi_face[side, f],
+          // the neighbour's with phi_face[1 - side, nf]
+          double tc[4] = {0.0, 0.0, 0.0, 0.0}, tn[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int j = 0; j < NE; ++j) {
+            const double cj = own[j * NQF + q];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) tc[s] = fma(cj, col[(own_node[j] * 4 + s) * EB], tc[s]);
+          }
+          double F[4], sp;
+          if (nb >= 0) {
+#pragma unroll
+            for (int j = 0; j < NE; ++j) {
+              const double l = oth[j * NQF + q];
+#pragma unroll
+              for (int s = 0; s < 4; ++s) tn[s] = fma(l, nbc[(j * 4 + s) * EB], tn[s]);
+            }
+            double Lt[4], Rt[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+              Lt[s] = side ? tn[s] : tc[s];
+              Rt[s] = side ? tc[s] : tn[s];
+            }
+            sp = interface_flux(Lt, Rt, nx, ny, ph, F);
+          } else {
+            const double p_back = (inst >= 0 && m.inst_p_back) ? __ldg(m.inst_p_back + inst) : ph.p_back;
+            sp = boundary_flux(tag, tc, nx, ny, ph, p_back, F);
+          }
+          smax = sp > smax ? sp : smax;
+          const double scale = jac * c_tab[S::O_WF + q];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) fw[(q * 4 + s) * EB] = (F[s] * scale) * coef;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < NQF; ++q)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) fw[(q * 4 + s) * EB] = 0.0;
+      }
+      smem[L::WAVE + f * EB + lane] = smax * len;
+    } else {
+      constexpr int n1 = PL::LATE;
+      if constexpr (n1 > 0) split_volume<K, P, AFF, NQV - n1, n1>(col, smem + L::FV + lane, m, e, active, rate, g);
+    }
+    __syncthreads();
+
+    // ---- phase A2: the other volume points, split evenly over the warps
+    for_part(r, [&](auto R) {
+      constexpr SplitRanges pr = PL::even(NQV - PL::LATE);
+      constexpr int q0 = pr.first[decltype(R)::value], nq = pr.count[decltype(R)::value];
+      if constexpr (nq > 0) split_volume<K, P, AFF, q0, nq>(col, smem + L::FV + lane, m, e, active, rate, g);
+    });
+    __syncthreads();
+
+    double wave = 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) wave += smem[L::WAVE + f * EB + lane];
+    if (w.wave && r == 0 && active) w.wave[e] = wave;
+
+    // ---- phase B: component s = r of every node.  The face lift first: the
+    // flux at face point q times this element's basis of its side of the face
+    // (the fused kernel's order: faces in turn, points in turn), then the
+    // volume sums.
+    const int s = r;
+    double acc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i] = 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const bool sd = (sides >> f) & 1;
+#pragma unroll
+      for (int q = 0; q < NQF; ++q) {
+        const double fwq = smem[L::LIFT + ((f * NQF + q) * 4 + s) * EB + lane];
+#pragma unroll
+        for (int j = 0; j < NE; ++j) {
+          const double c0v = pfe<K, P>(0, f, j, q), c1v = pfe<K, P>(1, f, j, q);
+          const int n = edge_node(K, P, f, j);
+          acc[n] = fma(sd ? c1v : c0v, fwq, acc[n]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NQV; ++q) {
+      const double fx = smem[L::FV + (q * 8 + s) * EB + lane];
+      const double fe = smem[L::FV + (q * 8 + 4 + s) * EB + lane];
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+        acc[i] = fma(tab<K, P>(S::O_WXI + i * NQV + q), fx, fma(tab<K, P>(S::O_WETA + i * NQV + q), fe, acc[i]));
+    }
+
+    if (w.op == OP_RESIDUAL) {
+      if (active) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) w.out[((int64_t)s * NP + i) * E + e] = acc[i];
+      }
+      return;  // every warp of the block leaves here: no barrier follows
+    }
+
+    double dt = 0.0;
+    if (stage && active) {
+      if (w.stage == 1) {
+        const double d = wave < FLOOR ? FLOOR : wave;
+        dt = w.dt_factor * 2.0 * __ldg(m.area + e) / d;
+        if (r == 0) w.dt[e] = dt;
+      } else {
+        dt = w.dt[e];
+      }
+    }
+    if (AFF) {
+      // rate -M^-1 R of component s from the reference table (M = det M_ref)
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        double ri = 0.0;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) ri = fma(tab<K, P>(S::O_MINV + i * NP + j), acc[j], ri);
+        if (!active) continue;
+        if (!stage) {
+          w.out[((int64_t)s * NP + i) * E + e] = ri;
+          continue;
+        }
+        const double v = col[(i * 4 + s) * EB];
+        double un;
+        if (w.stage == 1) {
+          const double rw = ri * ph.norm_w[s];
+          nrm = fma(rw, rw, nrm);
+          un = v + dt * ri;
+        } else {
+          const double u0 = __ldg(w.U0 + ((int64_t)s * NP + i) * E + e);
+          un = w.a * u0 + w.b * (v + dt * ri);
+        }
+        col[(i * 4 + s) * EB] = un;
+      }
+    } else {
+      // general geometry: the element's own inverse mass, by rows -- the
+      // projection sums move through shared memory (FV is free once every
+      // warp has read it)
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < NP; ++i) smem[L::FV + (i * 4 + s) * EB + lane] = acc[i];
+      __syncthreads();
+      for_part(r, [&](auto R) {
+        constexpr SplitRanges rr = PL::even(NP);
+        constexpr int i0 = rr.first[decltype(R)::value], ni = rr.count[decltype(R)::value];
+        if constexpr (ni > 0) {
+          double rv[ni][4];
+#pragma unroll
+          for (int k = 0; k < ni; ++k)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) rv[k][c] = 0.0;
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            double aj[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) aj[c] = smem[L::FV + (j * 4 + c) * EB + lane];
+#pragma unroll
+            for (int k = 0; k < ni; ++k) {
+              const double mij = active ? __ldg(m.minv + ((int64_t)(i0 + k) * NP + j) * E + e) : 0.0;
+#pragma unroll
+              for (int c = 0; c < 4; ++c) rv[k][c] = fma(mij, aj[c], rv[k][c]);
+            }
+          }
+          if (active) {
+#pragma unroll
+            for (int k = 0; k < ni; ++k) {
+              const int i = i0 + k;
+#pragma unroll
+              for (int c = 0; c < 4; ++c) {
+                const double ri = -rv[k][c];
+                if (!stage) {
+                  w.out[((int64_t)c * NP + i) * E + e] = ri;
+                  continue;
+                }
+                const double v = col[(i * 4 + c) * EB];
+                double un;
+                if (w.stage == 1) {
+                  const double rw = ri * ph.norm_w[c];
+                  nrm = fma(rw, rw, nrm);
+                  un = v + dt * ri;
+                } else {
+                  const double u0 = __ldg(w.U0 + ((int64_t)c * NP + i) * E + e);
+                  un = w.a * u0 + w.b * (v + dt * ri);
+                }
+                col[(i * 4 + c) * EB] = un;
+              }
+            }
+          }
+        }
+      });
+    }
+    if (!stage) return;  // rate: every warp leaves here
+  }
+
+  // ---- the new state is complete in shared memory
+  __syncthreads();
+  if (stage && w.stage == 1 && (w.norm_partial || w.elem_norm)) {
+    smem[L::NRM + r * EB + lane] = nrm;
+    __syncthreads();
+    double tot = 0.0;
+    if (r == 0) {
+#pragma unroll
+      for (int k = 0; k < SPLIT_T; ++k) tot += smem[L::NRM + k * EB + lane];
+      if (w.elem_norm && active) w.elem_norm[e] = tot;
+    }
+    if (w.norm_partial) block_sum_store<SPLIT_T>(tot, w.norm_partial + blockIdx.x);
+  }
+
+  // ---- phase C: the positivity limiter (limiter 1), every warp for its lane's element
+  int scaled = 0, repaired = 0;
+  double ub[4] = {0.0, 0.0, 0.0, 0.0}, theta = 1.0;
+  bool lim = false;
+  if (LIM && ph.limiter == 1 && P > 0) {
+    const bool do_lim = active;
+    double mw[NP];
+    if (do_lim) mean_weights<K, P, AFF>(m, e, mw);
+    auto cell_mean = [&]() {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ub[c] = 0.0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ub[c] = fma(mw[i], col[(i * 4 + c) * EB], ub[c]);
+    };
+    if (do_lim) cell_mean();
+    // last-resort repair of a non-physical cell average
+    const double rho_new = ub[0] < ph.rho_floor ? ph.rho_floor : ub[0];
+    const double e_min = ph.p_floor / (g - 1.0) + 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / rho_new;
+    const double rhoE_new = ub[3] < e_min ? e_min : ub[3];
+    const bool rep = do_lim && (ub[0] < ph.rho_floor || ub[3] < e_min);
+    if (__syncthreads_or(rep)) {
+      if (rep && (r == 0 || r == 3)) {
+        const double d = r == 0 ? rho_new - ub[0] : rhoE_new - ub[3];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) col[(i * 4 + r) * EB] += d;
+      }
+      __syncthreads();
+      if (rep) cell_mean();
+    }
+    repaired = rep ? 1 : 0;
+    double eps_r = 0.0, eps_p = 0.0;
+    bool probe = false;
+    if (do_lim) {
+      const double pbar = (g - 1.0) * (ub[3] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / ub[0]);
+      eps_r = ph.lim_fraction * ub[0];
+      eps_r = eps_r < 0.5 * ph.rho_floor ? 0.5 * ph.rho_floor : eps_r;
+      eps_p = ph.lim_fraction * pbar;
+      eps_p = eps_p < 0.5 * ph.p_floor ? 0.5 * ph.p_floor : eps_p;
+      // sufficient screen: bound every probe through the Lebesgue constant
+      double dev[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dev[c] = fmax(dev[c], fabs(col[(i * 4 + c) * EB] - ub[c]));
+      const double lam = ph.lebesgue;
+      const double rho_lo = ub[0] - lam * dev[0];
+      probe = true;
+      if (rho_lo >= eps_r) {
+        const double m_hi = sqrt(ub[1] * ub[1] + ub[2] * ub[2]) + lam * sqrt(dev[1] * dev[1] + dev[2] * dev[2]);
+        const double p_lo = (g - 1.0) * (ub[3] - lam * dev[3] - 0.5 * m_hi * m_hi / rho_lo);
+        if (p_lo >= eps_p) probe = false;
+      }
+    }
+    double rmin = 1e300, pmin = 1e300, tstar = 1e300;
+    if (__syncthreads_or(probe)) {
+      if (probe) {
+        for_part(r, [&](auto R) {
+          constexpr SplitRanges pp = PL::even(S::NPROBE);
+          constexpr int p0 = pp.first[decltype(R)::value], np = pp.count[decltype(R)::value];
+          if constexpr (np > 0)
+            split_probe<K, P, p0, np>(col, smem + L::SCR + r * 8 * EB + lane, ub, sides, eps_p, g, rmin, pmin, tstar);
+        });
+      }
+      smem[L::RED + (r * 3 + 0) * EB + lane] = rmin;
+      smem[L::RED + (r * 3 + 1) * EB + lane] = pmin;
+      smem[L::RED + (r * 3 + 2) * EB + lane] = tstar;
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < SPLIT_T; ++k) {
+        const double a = smem[L::RED + (k * 3 + 0) * EB + lane];
+        const double b = smem[L::RED + (k * 3 + 1) * EB + lane];
+        const double c = smem[L::RED + (k * 3 + 2) * EB + lane];
+        rmin = a < rmin ? a : rmin;
+        pmin = b < pmin ? b : pmin;
+        tstar = c < tstar ? c : tstar;
+      }
+    }
+    lim = probe && ((rmin < eps_r) || (pmin < eps_p));
+    if (lim && rmin < eps_r) {
+      const double gap = ub[0] - rmin;
+      theta = (ub[0] - eps_r) / (gap > 0.0 ? gap : 1.0);
+      theta = theta < 0.0 ? 0.0 : (theta > 1.0 ? 1.0 : theta);
+    }
+    // The reference bisects on min_x p(ubar + t (u(x) - ubar)) >= eps_p over
+    // [0, theta] (12 steps, src/spatial/limiter.py:151-178); p is concave along
+    // the segment, so the test is "t <= t*", replayed here on t* with the
+    // reference's midpoints.  A decision within 1e-7 theta of t* is re-taken
+    // pointwise, the probe points split over the warps (a block-uniform loop:
+    // every thread meets every barrier).
+    // the pointwise re-check: every thread meets its barriers
+    auto recheck = [&](bool need, double t, bool adm) -> bool {
+      if (__syncthreads_or(need)) {
+        const double pm = need ? split_pmin<K, P>(col, s_pfe, r, ub, t, sides, g) : 1e300;
+        smem[L::RED + r * EB + lane] = pm;
+        __syncthreads();
+        if (need) {
+          double mn = 1e300;
+#pragma unroll
+          for (int k = 0; k < SPLIT_T; ++k) {
+            const double v = smem[L::RED + k * EB + lane];
+            mn = v < mn ? v : mn;
+          }
+          adm = mn >= eps_p;
+        }
+      }
+      return adm;
+    };
+    if (__syncthreads_or(lim)) {
+      const bool adm0 = recheck(lim && fabs(theta - tstar) <= 1e-7 * theta, theta, theta < tstar);
+      const bool bis = lim && !adm0;
+      if (__syncthreads_or(bis)) {
+        double lo = 0.0, hi = theta;
+        for (int it = 0; it < ph.lim_steps; ++it) {
+          const double t = 0.5 * (lo + hi);
+          const bool adm = recheck(bis && fabs(t - tstar) <= 1e-7 * theta, t, t < tstar);
+          if (adm)
+            lo = t;
+          else
+            hi = t;
+        }
+        if (bis) theta = lo;
+      }
+    }
+    scaled = lim ? 1 : 0;
+  }
+
+  // ---- write the (limited) new state: warp r writes component r
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double v = col[(i * 4 + r) * EB];
+      if (lim) v = ub[r] + theta * (v - ub[r]);
+      w.out[((int64_t)r * NP + i) * E + e] = v;
+    }
+    if (w.flags && r == 0) w.flags[e] = (uint8_t)(scaled | (repaired << 1));
+  }
+  if (w.counters) {
+    const int ns = __syncthreads_count(r == 0 && scaled);
+    const int nr = __syncthreads_count(r == 0 && repaired);
+    if (threadIdx.x == 0) {
+      if (ns) atomicAdd(w.counters + 0, (unsigned long long)ns);
+      if (nr) atomicAdd(w.counters + 1, (unsigned long long)nr);
+    }
+  }
+}
+
+}  // namespace nzb

@@ -243,6 +243,7 @@ class DeviceMesh:
         m.edge_flux = self.edge_flux.data_ptr()
         m.edge_speed = self.edge_speed.data_ptr()
         m.edge_pass = 0
+        m.split = 1
         # Superbee limiter: each element's share of the domain's area and scratch
         if "area" in arrays:
             area = np.asarray(arrays["area"], float)
@@ -282,6 +283,17 @@ class DeviceMesh:
         if getattr(self, "elem_share", None) is not None:
             area = self.arrays["area"]
             self.elem_share.copy_(area / area.sum())
+
+    @property
+    def split(self) -> int:
+        return int(self.c.split) if self.c.split > 1 else 1
+
+    @split.setter
+    def split(self, threads: int) -> None:
+        """Threads per element of the forward kernels: 1, or 4 (orders >= 1)."""
+        if threads not in (1, 4):
+            raise ValueError("split takes 1 or 4 threads per element")
+        self.c.split = 4 if (threads == 4 and self.order > 0) else 1
 
     @property
     def edge_pass(self) -> bool:

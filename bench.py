@@ -217,8 +217,11 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500, ki
                 results[f"stage{k}_hllc"] = float(np.mean(stimes[k]))
         del bk
         torch.cuda.empty_cache()
-    # algorithmic bytes per element: state in/out, geometry (affine: inverse Jacobian and
-    # det; general: vertices and the inverse mass), connectivity, edges once
+    # algorithmic bytes per element: the state read and the result written (S = NP * 4 * 8 bytes each;
+    # stages 2 and 3 also read the step's start state), the element geometry (affine: inverse Jacobian and
+    # det, 40 B; general: the vertices, 64 B, and for rates and stages the inverse mass, NP^2 * 8 B), the
+    # connectivity (neighbour, edge and face code per face: 12 B each), every edge's normal, |dX/dsigma| and
+    # length once (32 B per edge), and the element's wave speed or local step (8 B; stage 1 also reads the area)
     S = NP * 4 * 8
     n_edge = ops.n_edges_total
     nf = 3 if kind == "tri" else 4

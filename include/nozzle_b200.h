@@ -83,6 +83,11 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * the element kernel lifts them; edge_pass = 0 evaluates the fluxes inside the
  * element kernel, from both sides.  Both give bit-identical results; which is
  * faster depends on the element kind, order and mesh size.
+ * split = 4 (orders >= 1) runs the element kernel with four threads per
+ * element -- faces and volume points split over a block's four warps, the
+ * projection by component, the limiter's probe points split -- and ignores
+ * edge_pass; split = 0 or 1 runs one thread per element.  It agrees with the
+ * one-thread kernels to round-off (a few sums associate differently).
  */
 typedef struct {
   int32_t kind;
@@ -108,6 +113,8 @@ typedef struct {
   const double* elem_share; /* (E) A_e / A_domain, for the Superbee limiter (limiter 2) */
   double* lim_means;        /* (4, E) scratch of the Superbee limiter */
   double* lim_scale;        /* (4) scratch of the Superbee limiter */
+  int32_t split;            /* threads per element of the forward kernels: 0 or 1, or 4 */
+  int32_t reserved_split;
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly
@@ -206,7 +213,11 @@ int nzb_norm(const double* A, int64_t n_elem, int np, const double* w4, double* 
  * n_elem is limited to 8,388,608; a larger n_elem is rejected with an error
  * and nothing is launched.  No call allocates or frees memory.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  All
+ * that device current; make that first call before any stream capture.  The
+ * address is kept per device ordinal for the life of the process, which
+ * assumes the device's primary context (the one the CUDA runtime and torch
+ * use) throughout: after cudaDeviceReset, or from another driver-API context
+ * on the same device, the kept address is not valid there.  All
  * calls share the array, which keeps the last call's partial sums -- each call
  * overwrites every slot it reads -- and calls that overlap on the GPU (other
  * streams, other host threads) race on it. */

@@ -410,6 +410,85 @@ def sweep_outcomes(n=256, seed=0, max_it=20000, workers=6):
     print("wrote sweep_reference.json")
 
 
+
+# the config-4 member whose gradient the GPU test checks: eight radial offsets,
+# Gaussian with sigma = 2 % of the throat half-height (numpy default_rng(4))
+CONFIG4 = dict(area_ratio=2.5, element="tri", order=2, refine=2, flux="ausmup", back_pressure_ratio=0.15)
+
+
+def config4_offsets(sigma=0.02, seed=4):
+    return np.random.default_rng(seed).normal(0.0, sigma, 8)
+
+
+def config4_fd(h=1e-6, tol=1e-12):
+    """Central differences of thrust w.r.t. the eight Bezier offsets of config 4, from the reference's solver.
+
+    The reference has no eight-offset wall.  In this generator process only,
+    its wall function is wrapped: for the smooth contour it returns the
+    reference's own smooth wall plus y_throat * sum_k B_{9,k+1}(s) offset_k
+    (degree-9 Bernstein polynomials of the diverging coordinate s, zero at both
+    ends), which is the eight-offset family the repository builds.  Every
+    forward solve is the reference's solve_nozzle (Numba backend) from its own
+    quasi-1D initial state, to a scaled residual of ``tol``; thrust is the
+    reference's objective (src/sensitivity.py:107-114): twice the outflow plus
+    inflow axial momentum flux through its own boundary_trace.
+    """
+    import json
+    import math
+
+    import src.geometry.contour as contour_mod
+    import src.geometry.mesh as mesh_mod
+    from src.api import solve_nozzle
+    from src.geometry.mesh import BoundaryTag
+    from src.post.postprocess import axial_momentum_flux, boundary_trace
+
+    orig = contour_mod.wall_half_height
+    current = {"off": np.zeros(8)}
+
+    def wall_bezier8(x, params, contour="bell", xp=np):
+        y = orig(x, params, contour, xp=xp)
+        if contour != "smooth":
+            return y
+        xi = xp.asarray(x) / params.get("length", 1.0)
+        x_th = params["throat_x"]
+        s = xp.clip((xi - x_th) / (1.0 - x_th), 0.0, 1.0)
+        bump = sum(math.comb(9, k + 1) * s ** (k + 1) * (1.0 - s) ** (8 - k) * current["off"][k] for k in range(8))
+        return y + params["throat_half_height"] * bump
+
+    contour_mod.wall_half_height = wall_bezier8
+    mesh_mod.wall_half_height = wall_bezier8
+
+    def thrust(off):
+        current["off"] = np.asarray(off, float)
+        res = solve_nozzle(contour="smooth", tolerance=tol, max_iterations=400_000, backend="numba", verbose=False,
+                           **CONFIG4)
+        if not res.converged:
+            raise RuntimeError(f"reference forward solve did not converge: {res.message}")
+        gam = res.flow.gamma
+        out = boundary_trace(res.U, res.operators, BoundaryTag.OUTFLOW)
+        inl = boundary_trace(res.U, res.operators, BoundaryTag.INFLOW)
+        return float(2.0 * (axial_momentum_flux(out, gam) + axial_momentum_flux(inl, gam))), int(res.iterations)
+
+    base = config4_offsets()
+    value, it0 = thrust(base)
+    grad, iters = [], [it0]
+    for k in range(8):
+        up, dn = base.copy(), base.copy()
+        up[k] += h
+        dn[k] -= h
+        tu, iu = thrust(up)
+        td, idn = thrust(dn)
+        grad.append((tu - td) / (2.0 * h))
+        iters += [iu, idn]
+        print(f"offset_{k}: {grad[-1]:.10e}")
+    contour_mod.wall_half_height = orig
+    mesh_mod.wall_half_height = orig
+    doc = {"case": CONFIG4, "offsets": base.tolist(), "step": h, "tolerance": tol, "thrust": value,
+           "gradient": grad, "iterations": iters}
+    with open(os.path.join(HERE, "config4_fd.json"), "w") as f:
+        json.dump(doc, f, indent=1)
+    print("wrote config4_fd.json")
+
 if __name__ == "__main__":
     import src  # noqa: F401  -- fails loudly when the reference is not on PYTHONPATH
 
@@ -432,3 +511,5 @@ if __name__ == "__main__":
         observables()
     if "continuation" in which:
         continuation_cases()
+    if "config4" in which:
+        config4_fd()

@@ -52,18 +52,37 @@ def test_table_sizes_agree_with_the_packer():
     assert lib.nzb_version() == 1
 
 
-def test_struct_layouts_match_the_header():
+STRUCTS = {"Mesh": "nzb_mesh", "Physics": "nzb_physics", "StageArgs": "nzb_stage_args", "Buffers": "nzb_buffers",
+           "BatchMarch": "nzb_batch_march", "AdjointArgs": "nzb_adjoint_args", "AdjointBuffers": "nzb_adjoint_buffers",
+           "AdjointMarch": "nzb_adjoint_march", "ObsArgs": "nzb_obs_args", "GeometryArgs": "nzb_geometry_args"}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes structure has the C compiler's size and field offsets for the header's struct."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
     capi = pkg("capi")
-    # 4 x int32 + 2 x int64 + 10 pointers
-    assert ctypes.sizeof(capi.Mesh) == 16 + 16 + 16 * 8
-    assert ctypes.sizeof(capi.Physics) == 3 * 8 + 8 + 9 * 8 + 4 * 8 + 8 + 4 * 8 + 8
-    assert ctypes.sizeof(capi.StageArgs) == 8 * 8 + 3 * 8 + 8
-    assert ctypes.sizeof(capi.BatchMarch) == 8 + 12 * 8 + 2 * 8 + 2 * 4
-    assert ctypes.sizeof(capi.AdjointArgs) == 8 + 11 * 8
-    assert ctypes.sizeof(capi.AdjointBuffers) == 9 * 8
-    assert ctypes.sizeof(capi.AdjointMarch) == 8 + 9 * 8 + 8 + 2 * 4
-    assert ctypes.sizeof(capi.ObsArgs) == 8 + 2 * 4 + 3 * 8 + 2 * 8 + 8
-    assert ctypes.sizeof(capi.GeometryArgs) == 3 * 8 + 16 * 8 + 4 * 8
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nozzle_b200.h"', "int main(void) {"]
+    for py, c in STRUCTS.items():
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        for name, _ in getattr(capi, py)._fields_:
+            lines.append(f'  printf("{py} {name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(line.split()[:2]): int(line.split()[2]) for line in out if line}
+    for py in STRUCTS:
+        cls = getattr(capi, py)
+        assert got[(py, "size")] == ctypes.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert got[(py, name)] == getattr(cls, name).offset, (py, name)
 
 
 def test_lebesgue_constant_bounds_probe_values():

@@ -18,6 +18,13 @@ FLUXES = ("roe", "hllc", "ausmup")
 TOL = 1e-12
 
 
+@pytest.fixture(params=["t1", "split4"], autouse=True)
+def variant(request, monkeypatch):
+    """Every test runs with one thread per element and with four (the split kernel)."""
+    monkeypatch.setenv("NZB_VARIANT", request.param)
+    return request.param
+
+
 def backend(ops, flow=None, opts=None, **kw):
     cfg = pkg("config")
     return pkg("backend").B200Backend(ops, flow or cfg.FlowConditions(), opts or cfg.SolverOptions(), **kw)
@@ -152,6 +159,7 @@ def test_edge_pass_is_bit_identical(cuda, kind, p, flux):
     ops, g = tiny_ops(kind, p)
     flow = pkg("config").FlowConditions(flux=flux, back_pressure_ratio=0.9)
     bk = backend(ops, flow)
+    bk.mesh.split = 1
     out = {}
     for ep in (False, True):
         bk.mesh.edge_pass = ep
@@ -161,3 +169,27 @@ def test_edge_pass_is_bit_identical(cuda, kind, p, flux):
         out[ep] = (R, wave, F, U1, res, flags)
     for a, b in zip(out[False], out[True]):
         assert np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
+
+
+@pytest.mark.parametrize("kind,p", [c for c in TINY if c[1] > 0])
+@pytest.mark.parametrize("flux", FLUXES)
+def test_split_agrees_with_one_thread(cuda, kind, p, flux, variant):
+    """Four threads per element against one: residual, rate, wave, a stage and its limited set, to round-off."""
+    if variant != "t1":
+        pytest.skip("compares both variants itself")
+    ops, g = tiny_ops(kind, p)
+    flow = pkg("config").FlowConditions(flux=flux, back_pressure_ratio=0.9)
+    for general in geometries(kind):
+        bk = backend(ops, flow, force_general=general)
+        out = {}
+        for split in (1, 4):
+            bk.mesh.split = split
+            R, wave = bk.residual(g["U"])
+            F, _ = bk.rate(g["U"])
+            U1, res, flags = bk.step_record(g["U"])
+            L, lflags = bk.limit_flags(g["U_bad"])
+            out[split] = (R, wave, F, U1, res, flags, L, lflags)
+        a, b = out[1], out[4]
+        for x, y in zip(a[:5] + a[6:7], b[:5] + b[6:7]):
+            assert rel(y, x) < 1e-13
+        assert np.array_equal(a[5], b[5]) and np.array_equal(a[7], b[7])

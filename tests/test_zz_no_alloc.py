@@ -50,6 +50,17 @@ def test_noalloc_norm_matches_the_allocating_one(cuda):
         assert abs(got - expect) <= 1e-13 * expect
 
 
+def test_noalloc_norm_at_its_largest_size(cuda):
+    """n_elem = 8,388,608 fills every slot of the fixed array (np = 1: a 256 MB input)."""
+    capi = pkg("capi")
+    lib = capi.load()
+    for _ in range(2):
+        ref, got, expect = _norm_both(cuda, lib, capi, 8_388_608, 1, 4)
+        assert got == ref, (got, ref)
+        assert abs(got - expect) <= 1e-12 * expect
+    cuda.cuda.empty_cache()
+
+
 def test_noalloc_norm_refuses_an_oversized_mesh(cuda):
     capi = pkg("capi")
     lib = capi.load()
