@@ -10,8 +10,9 @@ The forward kernels come in three variants:
                   elements: faces and volume points split over the warps, the
                   projection by component, the limiter's probe scan split).
 
-They evaluate the same formulas; ``t1`` and ``t1_edge`` agree bit for bit on
-a step, ``split4`` to round-off (a few sums associate differently).  Over a
+They evaluate the same formulas and agree to round-off on a step (the
+compiler contracts multiply-adds differently in different kernels, and
+``split4`` associates a few sums differently).  Over a
 long march round-off differences grow, so the variant is fixed per (kind,
 order), never per mesh: a single solve and a batch of the same element type
 run the same kernels and give the same bits.

@@ -157,6 +157,11 @@ __device__ __forceinline__ void probe_scan(const A& u, const double (&ub)[4], in
     rmin = w[0] < rmin ? w[0] : rmin;
     const double pp = pressure_at(w, g);
     pmin = pp < pmin ? pp : pmin;
+    // when the segment starts inside the bound (c > 0: the cell mean's
+    // pressure exceeds eps_p), a point with positive density that meets the
+    // bound at t = 1 cannot bind on (0, 1] (p is concave along the segment);
+    // t <= theta <= 1 in every comparison with t*, so its root is not needed
+    if (c > 0.0 && !(pp < eps_p) && w[0] > 0.0) continue;
     const double d0 = w[0] - ub[0], d1 = w[1] - ub[1], d2 = w[2] - ub[2], d3 = w[3] - ub[3];
     const double a = d3 * d0 - 0.5 * (d1 * d1 + d2 * d2);
     const double b = ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0;
@@ -380,7 +385,7 @@ __device__ __forceinline__ int face_sides(const nzb_mesh& m, int64_t e) {
 // contiguous, read as whole 32-byte sectors by both its elements) and max_q s_q
 // (edge_speed), the reference's edge_pass (src/backends/_numba_kernels.py:
 // 484-583).  The element kernel with EP = true lifts them.  The arithmetic is
-// the fused kernel's, so both variants give bit-identical residuals.
+// the fused kernel's, so both variants agree to round-off.
 template <int K, int P>
 __global__ void __launch_bounds__(128, NZB_MINB_EDGE) k_edge(const nzb_mesh m, const nzb_physics ph, const double* __restrict__ V) {
   using S = Shape<K, P>;

@@ -27,34 +27,28 @@ __device__ __forceinline__ T floor_at(const T& x, double f) {
 
 template <class T>
 struct PrimT {
-  T rho, vx, vy, p, H;
+  T rho, vx, vy, p, H, inv;  // inv = 1 / rho
 };
 using Prim = PrimT<double>;
 
+// Primitives with one reciprocal of the (floored) density: vx = U1 (1/rho)
+// differs from the reference's U1 / rho in the last bit at most, and saves
+// two divisions -- each an iterative sequence on the FP64 pipe -- per state,
+// which is most of a face flux's cost.
 template <class T>
 __device__ __forceinline__ PrimT<T> primitives(const T* U, double g) {
   PrimT<T> s;
   s.rho = floor_at(U[0], FLOOR);
-  s.vx = U[1] / s.rho;
-  s.vy = U[2] / s.rho;
+  s.inv = 1.0 / s.rho;
+  s.vx = U[1] * s.inv;
+  s.vy = U[2] * s.inv;
   s.p = floor_at((g - 1.0) * (U[3] - 0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy)), FLOOR);
-  s.H = (U[3] + s.p) / s.rho;
+  s.H = (U[3] + s.p) * s.inv;
   return s;
 }
 
-// The same primitives with one division: vx = U1 (1/rho) differs from U1 / rho
-// in the last bit at most.  Used for the volume-point fluxes, which feed only
-// the weak-form projection, never a branch.
-__device__ __forceinline__ Prim primitives_fast(const double* U, double g) {
-  Prim s;
-  s.rho = floor_at(U[0], FLOOR);
-  const double inv = 1.0 / s.rho;
-  s.vx = U[1] * inv;
-  s.vy = U[2] * inv;
-  s.p = floor_at((g - 1.0) * (U[3] - 0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy)), FLOOR);
-  s.H = (U[3] + s.p) * inv;
-  return s;
-}
+// The volume-point primitives (feeding only the weak-form projection).
+__device__ __forceinline__ Prim primitives_fast(const double* U, double g) { return primitives(U, g); }
 
 // Every function below takes each operand group with its own scalar type --
 // the two traces (TL, TR), the normal (TN), the back pressure (TP) -- so that
@@ -95,10 +89,10 @@ __device__ __forceinline__ TF roe_flux(const TL* UL, const TR* UR, const TN& nx,
   normal_flux(R, nx, ny, FR);
   const TL sL = sqrt(L.rho);
   const TR sR = sqrt(R.rho);
-  const auto den = sL + sR;
-  const auto vx = (sL * L.vx + sR * R.vx) / den;
-  const auto vy = (sL * L.vy + sR * R.vy) / den;
-  const auto H = (sL * L.H + sR * R.H) / den;
+  const auto iden = 1.0 / (sL + sR);
+  const auto vx = (sL * L.vx + sR * R.vx) * iden;
+  const auto vy = (sL * L.vy + sR * R.vy) * iden;
+  const auto H = (sL * L.H + sR * R.H) * iden;
   const auto q2 = vx * vx + vy * vy;
   const auto c = sqrt(floor_at((g - 1.0) * (H - 0.5 * q2), FLOOR));
   const auto vn = vx * nx + vy * ny;
@@ -112,8 +106,9 @@ __device__ __forceinline__ TF roe_flux(const TL* UL, const TR* UR, const TN& nx,
   const auto G1 = (g - 1.0) * (0.5 * q2 * d0 - vx * d1 - vy * d2 + d3);
   const auto G2 = -vn * d0 + d1 * nx + d2 * ny;
   const auto s1 = 0.5 * (l1 + l2), s2 = 0.5 * (l1 - l2);
-  const auto C1 = (G1 / (c * c)) * (s1 - l3) + (G2 / c) * s2;
-  const auto C2 = (G1 / c) * s2 + (s1 - l3) * G2;
+  const auto ic = 1.0 / c;
+  const auto C1 = (G1 * (ic * ic)) * (s1 - l3) + (G2 * ic) * s2;
+  const auto C2 = (G1 * ic) * s2 + (s1 - l3) * G2;
   F[0] = 0.5 * (FL[0] + FR[0]) - 0.5 * (l3 * d0 + C1);
   F[1] = 0.5 * (FL[1] + FR[1]) - 0.5 * (l3 * d1 + C1 * vx + C2 * nx);
   F[2] = 0.5 * (FL[2] + FR[2]) - 0.5 * (l3 * d2 + C1 * vy + C2 * ny);
@@ -134,14 +129,14 @@ __device__ __forceinline__ TF hllc_flux(const TL* UL, const TR* UR, const TN& nx
   const PrimT<TR> R = primitives(UR, g);
   const auto vnL = L.vx * nx + L.vy * ny;
   const auto vnR = R.vx * nx + R.vy * ny;
-  const TL aL = sqrt(floor_at(g * L.p / L.rho, FLOOR));
-  const TR aR = sqrt(floor_at(g * R.p / R.rho, FLOOR));
+  const TL aL = sqrt(floor_at(g * L.p * L.inv, FLOOR));
+  const TR aR = sqrt(floor_at(g * R.p * R.inv, FLOOR));
   const TL sL = sqrt(L.rho);
   const TR sR = sqrt(R.rho);
-  const auto den = sL + sR;
-  const auto vx = (sL * L.vx + sR * R.vx) / den;
-  const auto vy = (sL * L.vy + sR * R.vy) / den;
-  const auto H = (sL * L.H + sR * R.H) / den;
+  const auto iden = 1.0 / (sL + sR);
+  const auto vx = (sL * L.vx + sR * R.vx) * iden;
+  const auto vy = (sL * L.vy + sR * R.vy) * iden;
+  const auto H = (sL * L.H + sR * R.H) * iden;
   const auto vt = vx * nx + vy * ny;
   const auto at = sqrt(floor_at((g - 1.0) * (H - 0.5 * (vx * vx + vy * vy)), FLOOR));
   TF SL = fmin(vnL - aL, vt - at);
@@ -171,7 +166,7 @@ __device__ __forceinline__ TF hllc_flux(const TL* UL, const TR* UR, const TN& nx
   const TF SM = (R.rho * vnR * (SR - vnR) - L.rho * vnL * (SL - vnL) + L.p - R.p) / dm;
   // one side's star state: contact normal speed, own tangential velocity
   const bool left = SM >= 0.0;
-  const PrimT<TM> K = left ? PrimT<TM>{L.rho, L.vx, L.vy, L.p, L.H} : PrimT<TM>{R.rho, R.vx, R.vy, R.p, R.H};
+  const PrimT<TM> K = left ? PrimT<TM>{L.rho, L.vx, L.vy, L.p, L.H, L.inv} : PrimT<TM>{R.rho, R.vx, R.vy, R.p, R.H, R.inv};
   TM UK[4];
   TF FK[4];
 #pragma unroll
@@ -185,7 +180,7 @@ __device__ __forceinline__ TF hllc_flux(const TL* UL, const TR* UR, const TN& nx
   const TF rs = K.rho * fac;
   const TF vxs = K.vx + (SM - vn) * nx;
   const TF vys = K.vy + (SM - vn) * ny;
-  const TF Es = UK[3] / K.rho + (SM - vn) * (SM + K.p / guard(K.rho * (S - vn)));
+  const TF Es = UK[3] * K.inv + (SM - vn) * (SM + K.p / guard(K.rho * (S - vn)));
   F[0] = FK[0] + S * (rs - UK[0]);
   F[1] = FK[1] + S * (rs * vxs - UK[1]);
   F[2] = FK[2] + S * (rs * vys - UK[2]);
@@ -201,17 +196,18 @@ __device__ __forceinline__ TF ausm_up_flux(const TL* UL, const TR* UR, const TN&
   const PrimT<TR> R = primitives(UR, g);
   const auto vnL = L.vx * nx + L.vy * ny;
   const auto vnR = R.vx * nx + R.vy * ny;
-  const TL aL = sqrt(g * L.p / L.rho);
-  const TR aR = sqrt(g * R.p / R.rho);
+  const TL aL = sqrt(g * L.p * L.inv);
+  const TR aR = sqrt(g * R.p * R.inv);
   const auto ah = 0.5 * (aL + aR), rh = 0.5 * (L.rho + R.rho);
-  const auto mL = vnL / ah, mR = vnR / ah;
+  const auto iah = 1.0 / ah;
+  const auto mL = vnL * iah, mR = vnR * iah;
   const auto mb2 = 0.5 * (mL * mL + mR * mR);
   const auto pL2 = 0.25 * ((mL + 1.0) * (mL + 1.0)), mL2 = -0.25 * ((mL - 1.0) * (mL - 1.0));
   const auto pR2 = 0.25 * ((mR + 1.0) * (mR + 1.0)), mR2 = -0.25 * ((mR - 1.0) * (mR - 1.0));
   const auto m4p = fabs(mL) >= 1.0 ? 0.5 * (mL + fabs(mL)) : pL2 * (1.0 - 16.0 * BETA * mL2);
   const auto m4m = fabs(mR) >= 1.0 ? 0.5 * (mR - fabs(mR)) : mR2 * (1.0 + 16.0 * BETA * pR2);
   const auto dif = 1.0 - mb2;
-  const TF uh = ah * (m4p + m4m) + KP * (dif < 0.0 ? like(dif, 0.0) : dif) * (L.p - R.p) / (rh * ah);
+  const TF uh = ah * (m4p + m4m) + KP * (dif < 0.0 ? like(dif, 0.0) : dif) * (L.p - R.p) * iah / rh;
   const auto p5p = fabs(mL) >= 1.0 ? like(mL, mL > 0.0 ? 1.0 : 0.0) : pL2 * ((2.0 - mL) - 16.0 * ALPHA * mL * mL2);
   const auto p5m = fabs(mR) >= 1.0 ? like(mR, mR > 0.0 ? 0.0 : 1.0) : mR2 * ((-2.0 - mR) + 16.0 * ALPHA * mR * pR2);
   const TF ph = p5p * L.p + p5m * R.p + KU * p5p * p5m * rh * ah * (vnL - vnR);

@@ -268,8 +268,13 @@ __device__ __forceinline__ void split_probe(const double* col, double* scr, cons
         const double pp = pressure_at(w[k], g);
         pmin = pp < pmin ? pp : pmin;
         const double d0 = w[k][0] - ub[0], d1 = w[k][1] - ub[1], d2 = w[k][2] - ub[2], d3 = w[k][3] - ub[3];
-        scr[(2 * k) * SPLIT_EB] = d3 * d0 - 0.5 * (d1 * d1 + d2 * d2);
-        scr[(2 * k + 1) * SPLIT_EB] = ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0;
+        // when the segment starts inside the bound (c > 0), a point with
+        // positive density that meets the pressure bound at t = 1 cannot bind
+        // on (0, 1] (p is concave along the segment): its root is never
+        // compared, so it is marked skipped (a = b = 1)
+        const bool binds = !(c > 0.0) || pp < eps_p || !(w[k][0] > 0.0);
+        scr[(2 * k) * SPLIT_EB] = binds ? d3 * d0 - 0.5 * (d1 * d1 + d2 * d2) : 1.0;
+        scr[(2 * k + 1) * SPLIT_EB] = binds ? ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0 : 1.0;
       }
     }
 #pragma unroll 1

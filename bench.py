@@ -58,16 +58,8 @@ def pkg(name=""):
 
 # ------------------------------------------------------------------ workloads
 def microbench_state(n_elem, nbf, gamma=1.4, seed=0):
-    rng = np.random.default_rng(seed)
-    shape = (n_elem, nbf)
-    rho = rng.lognormal(0.0, 0.3, shape)
-    mach = rng.uniform(0.2, 3.0, shape)
-    ang = rng.uniform(0.0, 2.0 * np.pi, shape)
-    p = rng.lognormal(0.0, 0.5, shape)
-    a = np.sqrt(gamma * p / rho)
-    vx, vy = mach * a * np.cos(ang), mach * a * np.sin(ang)
-    E = p / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy)
-    return np.ascontiguousarray(np.stack([rho, rho * vx, rho * vy, E], -1))
+    """The microbenchmark's seeded per-node states (the package's generator, so tests draw the same ones)."""
+    return pkg("autotune").random_states(n_elem, nbf, gamma, seed)
 
 
 def microbench_case(nx=1000, nr=500, kind="tri", order=3):

@@ -81,7 +81,8 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * edge_pass = 1 splits every residual / stage into two launches: one thread
  * per edge evaluates each edge's fluxes once (the reference's edge_pass), then
  * the element kernel lifts them; edge_pass = 0 evaluates the fluxes inside the
- * element kernel, from both sides.  Both give bit-identical results; which is
+ * element kernel, from both sides.  Both evaluate the same formulas and agree
+ * to round-off (the compiler may contract multiply-adds differently); which is
  * faster depends on the element kind, order and mesh size.
  * split = 4 (orders >= 1) runs the element kernel with four threads per
  * element -- faces and volume points split over a block's four warps, the

@@ -9,6 +9,8 @@ are exact to round-off; the summation orders differ).
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -158,15 +160,33 @@ def test_batched_gradients_match_one_at_a_time(cuda):
             assert abs(r.grad[k] - grad[k]) <= 1e-7 * max(abs(grad[k]), 1e-8), (k, r.grad[k], grad[k])
 
 
-def test_bezier8_shape_gradient_matches_central_differences(cuda):
-    """Eight-offset wall, AR 2.5, p = 2 triangles, refine 2, AUSM+-up: adjoint vs central differences."""
+def test_bezier8_shape_gradient_matches_the_reference_fd(cuda):
+    """Config 4: eight-offset wall, AR 2.5, p = 2 triangles, refine 2, AUSM+-up.
+
+    The adjoint gradient of thrust w.r.t. all eight offsets against central
+    differences (h = 1e-6) of the reference's own forward solver
+    (tests/golden/config4_fd.json, made by make_golden.py with the eight-offset
+    wall patched into the reference in the generating process only; its forward
+    solves converged to a scaled residual of 1e-12).  Both the forward
+    tolerance and the differences' own noise (a converged thrust to ~1e-13
+    over 2h) limit the agreement to about 1e-5 of the largest component.
+    """
+    import json
+
+    from conftest import GOLDEN
+
     ad = pkg("adjoint")
-    m0 = bezier8_members(1, seed=4)[0]
-    dc = ad.differentiable_case(contour="bezier8", area_ratio=2.5, order=2, refine=2, flux="ausmup",
-                                back_pressure_ratio=0.15, tolerance=1e-11, offsets=tuple(m0.values()))
-    names = ("offset_1", "offset_5")
+    with open(os.path.join(GOLDEN, "config4_fd.json")) as fh:
+        ref = json.load(fh)
+    c = ref["case"]
+    dc = ad.differentiable_case(contour="bezier8", area_ratio=c["area_ratio"], order=c["order"], refine=c["refine"],
+                                flux=c["flux"], back_pressure_ratio=c["back_pressure_ratio"], tolerance=1e-12,
+                                offsets=tuple(ref["offsets"]))
+    names = tuple(f"offset_{k}" for k in range(8))
     value, grad, fwd = dc.value_and_gradient("thrust", names=names, adjoint_tolerance=1e-10)
     assert fwd.converged
-    fd = ad.finite_difference_gradient(dc, "thrust", names=names, step=1e-6)
-    for k in names:
-        assert abs(grad[k] - fd[k]) <= 1e-4 * abs(fd[k]) + 1e-9, (k, grad[k], fd[k])
+    assert abs(value - ref["thrust"]) <= 1e-9 * abs(ref["thrust"])
+    fd = np.asarray(ref["gradient"])
+    adj = np.array([grad[k] for k in names])
+    scale = np.abs(fd).max()
+    assert np.abs(adj - fd).max() <= 2e-5 * scale, (adj, fd)

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import TINY, golden, pkg, rel, tiny_ops
+from conftest import TINY, assert_step_agrees, golden, pkg, rel, roundoff_spread, tiny_ops
 from oracle import dg_oracle as orc
 
 pytestmark = pytest.mark.gpu
@@ -102,7 +102,9 @@ def test_microbench_distribution(cuda, flux):
     R, wave = bk.residual(g["U"])
     assert rel(R, g[f"R_{flux}"]) < TOL and rel(wave, g[f"wave_{flux}"]) < TOL
     V, res, flags = bk.step_record(g["U"].copy())
-    assert rel(V, g[f"step_{flux}"]) < TOL
+    stepper = lambda U: orc.Stepper(ops, bk.flow, bk.opts).run(U, 1)[0]  # noqa: E731
+    _, spread = roundoff_spread(stepper, g["U"])
+    assert_step_agrees(V, g[f"step_{flux}"], spread)
     assert abs(res - g[f"step_{flux}_res"]) <= 1e-12 * g[f"step_{flux}_res"]
     assert np.array_equal(flags & 1 > 0, g[f"step_{flux}_limited"])
     run, res2 = bk.run(g["U"].copy(), 1, "ssprk3")
@@ -152,10 +154,8 @@ def test_norm_matches_the_oracle(cuda):
 
 @pytest.mark.parametrize("kind,p", TINY)
 @pytest.mark.parametrize("flux", FLUXES)
-def test_edge_pass_is_bit_identical(cuda, kind, p, flux):
-    """The edge-pass variant and the fused variant give the same bits: residual, rate, wave and a stage."""
-    import torch
-
+def test_edge_pass_agrees_with_the_fused_kernel(cuda, kind, p, flux):
+    """The edge-pass and fused variants: residual, rate, wave and a stage to round-off, identical limited sets."""
     ops, g = tiny_ops(kind, p)
     flow = pkg("config").FlowConditions(flux=flux, back_pressure_ratio=0.9)
     bk = backend(ops, flow)
@@ -167,8 +167,10 @@ def test_edge_pass_is_bit_identical(cuda, kind, p, flux):
         F, _ = bk.rate(g["U"])
         U1, res, flags = bk.step_record(g["U"])
         out[ep] = (R, wave, F, U1, res, flags)
-    for a, b in zip(out[False], out[True]):
-        assert np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
+    a, b = out[False], out[True]
+    for x, y in zip(a[:5], b[:5]):
+        assert rel(y, x) < 1e-13
+    assert np.array_equal(a[5], b[5])
 
 
 @pytest.mark.parametrize("kind,p", [c for c in TINY if c[1] > 0])
