@@ -243,9 +243,11 @@ SWEEP_POINTS = 256
 SWEEP_SEED = 0
 
 
-def sweep_workload(max_iterations, n_points=SWEEP_POINTS):
+def sweep_workload(max_iterations, n_points=SWEEP_POINTS, rank=0, world=1):
+    """This rank's share of one sweep of ``n_points * world`` design points (seed 0): points rank, rank + world, ...
+    (with one rank, the whole ``n_points``-point sweep)."""
     sweep = pkg("sweep")
-    points = sweep.sample_points(n_points, SWEEP_SEED)
+    points = pkg("replicas").partition(sweep.sample_points(n_points * world, SWEEP_SEED), rank, world)
     insts, index, refused = sweep.build_instances(points, max_iterations=max_iterations)
     return points, insts, index, refused
 
@@ -482,7 +484,7 @@ def run_ours(args, rank, world, torch, dist):
     capi = pkg("capi")
     BatchSolver = pkg("batch").BatchSolver
     peak, peak_kind = load_peaks()
-    points, insts, index, refused = sweep_workload(args.max_iterations, args.points)
+    points, insts, index, refused = sweep_workload(args.max_iterations, args.points, rank, world)
     solver = BatchSolver(insts)
     flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream()
@@ -518,11 +520,17 @@ def run_ours(args, rank, world, torch, dist):
     t_rank = float(np.sum(times))
     replicas = pkg("replicas")
     t_max = replicas.max_over_ranks(t_rank, dist, "cuda")
-    value = replicas.whole_job_rate(n_conv * args.steps, world, t_max)
-    outcomes = {}
-    for r in res:
-        outcomes[r.status] = outcomes.get(r.status, 0) + 1
-    outcomes["refused"] = len(refused)
+    # host-side gather of the ranks' tallies (no data-path collective)
+    statuses = ("converged", "max_iterations", "stalled", "diverged", "non-finite", "running")
+    tally = [n_conv, len(insts), len(refused), int(solver.n_elem)] + [sum(r.status == s for r in res) for s in statuses]
+    tally = [int(round(v)) for v in replicas.sum_over_ranks(tally, dist, "cuda")]
+    n_conv_all, n_built_all, n_refused_all, n_elem_all = tally[:4]
+    value = replicas.whole_job_rate(n_conv_all * args.steps, t_max)
+    outcomes = {s: n for s, n in zip(statuses, tally[4:]) if n}
+    other = n_built_all - sum(tally[4:])
+    if other:
+        outcomes["other"] = other
+    outcomes["refused"] = n_refused_all
 
     # end to end: set-up from host arrays, march, every state and status back
     e2e_t, h2d, d2h = [], 0, 0
@@ -541,7 +549,7 @@ def run_ours(args, rank, world, torch, dist):
         # statuses, iterations, residuals, the observable sums, and one 4-byte read per chunk
         d2h = (4 * 2 + 8 * 2) * len(out) + 8 * pkg("capi").NOBS * len(perf) + 4 * sv.chunks
         del sv
-    e2e_value = world * n_conv / float(np.mean(e2e_t))
+    e2e_value = replicas.whole_job_rate(n_conv_all, replicas.max_over_ranks(float(np.mean(e2e_t)), dist, "cuda"))
 
     # plain (one solve at a time) vs batched on the same subset
     sub = insts[:: args.plain_stride]
@@ -619,12 +627,13 @@ def run_ours(args, rank, world, torch, dist):
         "dtype": "f64",
         "data": "synthetic: sampled operating points (seed 0) on the reference's own mesh generator and quasi-1D "
                 "initial states, built on the host",
-        "config": {"workload": f"design sweep: {len(points)} points, {len(insts)} built, {len(refused)} refused "
-                               f"(shock in nozzle); tri/quad p 1-3 refine 1-3, bell contour, HLLC, positivity "
+        "config": {"workload": f"design sweep: {args.points * world} points, {n_built_all} built, {n_refused_all} "
+                               f"refused (shock in nozzle); tri/quad p 1-3 refine 1-3, bell contour, HLLC, positivity "
                                f"limiter, tol 1e-10, cap {args.max_iterations} iterations",
-                   "elements": int(solver.n_elem), "buckets": len(solver.meshes), "outcomes": outcomes,
-                   "converged_per_step": int(n_conv), "l2": "flushed (256 MB write) before each sweep",
-                   "parallelism": f"replicas x{world}"},
+                   "elements": n_elem_all, "buckets_rank0": len(solver.meshes), "outcomes": outcomes,
+                   "converged_per_step": n_conv_all, "l2": "flushed (256 MB write) before each sweep",
+                   "parallelism": (f"sweep of {args.points * world} points partitioned over {world} GPUs "
+                                   f"({args.points} each, points r::{world})" if world > 1 else "1 GPU")},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "path": "BatchSolver(host instances) -> run() -> results() + observables()"},
         "plain": plain,
