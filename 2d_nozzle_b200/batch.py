@@ -73,9 +73,6 @@ class BatchSolver:
                 raise ValueError("every instance of a batch must share the march options")
             if inst.flow.flux not in FLUX_IDS:
                 raise NotImplementedError(f"flux {inst.flow.flux!r}")
-            if o.limiter == "superbee":
-                raise NotImplementedError("the Superbee limiter's domain-wide scale is per solve: batch with "
-                                          "limiter='positivity' or 'none'")
         self.opts = opts0
         dev = torch.device(device if device is not None else "cuda")
         self.device = dev
@@ -124,6 +121,21 @@ class BatchSolver:
                 l_off += E_i
             self._keep.append(torch.as_tensor(elem_inst, device=dev))
             dm.elem_inst_t = self._keep[-1]
+            if opts0.limiter == "superbee":
+                # each instance is limited against its own domain: area shares and the maximum of
+                # its cell averages per instance (4 numbers each)
+                area = np.asarray(arrays["area"], float)
+                share = np.empty_like(area)
+                l_off = 0
+                for part in parts:
+                    E_i = part["n_elem"]
+                    share[l_off:l_off + E_i] = area[l_off:l_off + E_i] / area[l_off:l_off + E_i].sum()
+                    l_off += E_i
+                dm.elem_share = torch.as_tensor(share, device=dev)
+                dm.lim_scale = torch.zeros(4 * n, dtype=torch.float64, device=dev)
+                dm.c.elem_share = dm.elem_share.data_ptr()
+                dm.c.lim_scale = dm.lim_scale.data_ptr()
+                dm.c.n_inst = n
             S = [dm.state() for _ in range(3)]
             dt = torch.zeros(dm.E, dtype=torch.float64, device=dev)
             U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])

@@ -45,7 +45,7 @@ class Mesh(C.Structure):
         ("lim_means", P),
         ("lim_scale", P),
         ("split", I32),
-        ("reserved_split", I32),
+        ("n_inst", I32),
     ]
 
 

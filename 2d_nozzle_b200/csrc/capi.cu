@@ -96,7 +96,8 @@ static int dispatch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cud
   if (m.edge_pass && (reinterpret_cast<uintptr_t>(m.edge_flux) & 15) != 0)
     return fail("edge_flux must be 16-byte aligned");
   if (ph.limiter == 2 && m.order > 0 && (w.op == OP_STAGE || w.op == OP_LIMIT)) {
-    if (m.elem_inst) return fail("the Superbee limiter applies to a mesh of one instance");
+    if (m.elem_inst && (m.n_inst < 1 || !m.inst_status))
+      return fail("the Superbee limiter in a batch needs n_inst (lim_scale holds 4 per instance) and inst_status");
     if (!m.elem_share || !m.lim_means || !m.lim_scale)
       return fail("the Superbee limiter needs elem_share, lim_means and lim_scale");
   }

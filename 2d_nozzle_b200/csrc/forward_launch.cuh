@@ -8,8 +8,8 @@
 //                  fluxes lifted from the edge array;
 //   otherwise      k_element: one thread per element, fluxes from both sides.
 // With the Superbee limiter (limiter 2) the element kernel leaves the stage
-// unlimited and three passes follow (cell means, their maximum, the slope
-// limiter with the positivity limiter).
+// unlimited and three passes follow (cell means, their maximum -- per
+// instance in a batch -- and the slope limiter with the positivity limiter).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -25,7 +25,10 @@ cudaError_t superbee_passes(const nzb_mesh& m, const nzb_physics& ph, const doub
                             unsigned long long* counters, uint8_t* flags, cudaStream_t st) {
   const unsigned nb = (unsigned)((m.n_elem + 127) / 128);
   k_cell_means<K, P, AFF><<<nb, 128, 0, st>>>(m, V, m.lim_means);
-  k_lim_scale<<<1, 1024, 0, st>>>(m.lim_means, m.n_elem, m.lim_scale);
+  if (m.elem_inst)
+    k_lim_scale_inst<<<nb, 128, 0, st>>>(m.lim_means, m.n_elem, m.elem_inst, m.lim_scale);
+  else
+    k_lim_scale<<<1, 1024, 0, st>>>(m.lim_means, m.n_elem, m.lim_scale);
   k_superbee<K, P, AFF><<<nb, 128, 0, st>>>(m, ph, V, out, counters, flags);
   return cudaGetLastError();
 }

@@ -12,8 +12,14 @@
 // as apply_limiter does.  Three passes, since the threshold needs a maximum
 // over the whole domain and the jumps need the neighbours' cell averages:
 //   k_cell_means   ubar of every element;
-//   k_lim_scale    max_e |ubar_s| per component (one block, order-free);
+//   k_lim_scale    max_e |ubar_s| per component (one block, order-free), or
+//   k_lim_scale_inst  the same per instance of a batch (the maximum of the
+//                  bit patterns of non-negative doubles, by atomics: exact and
+//                  order-free);
 //   k_superbee     the factor, the scaling and the positivity limiter.
+// In a batch every instance is limited against its own domain (its own
+// maximum and area shares, as its one-at-a-time solve would be), and the
+// elements of retired instances are left untouched.
 #pragma once
 #include "element.cuh"
 
@@ -36,6 +42,9 @@ __global__ void __launch_bounds__(128) k_cell_means(const nzb_mesh m, const doub
   constexpr int NP = S::NP;
   const int64_t E = m.n_elem;
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // a batch's per-instance maxima start from zero (k_lim_scale_inst follows on the same stream)
+  if (m.elem_inst && blockIdx.x == 0)
+    for (int k = threadIdx.x; k < 4 * m.n_inst; k += blockDim.x) m.lim_scale[k] = 0.0;
   if (e >= E) return;
   double mw[NP];
   mean_weights<K, P, AFF>(m, e, mw);
@@ -71,6 +80,33 @@ static __global__ void __launch_bounds__(1024) k_lim_scale(const double* __restr
   }
 }
 
+// scale[4 i + s] = max over instance i's elements of |means[s, e]|.  Values
+// are non-negative, so their bit patterns order as the values do; NaN is
+// dropped, as fmax drops it in k_lim_scale.  A warp whose elements all belong
+// to one instance reduces first and issues one atomic per component.
+static __global__ void __launch_bounds__(128) k_lim_scale_inst(const double* __restrict__ means, int64_t E,
+                                                               const int32_t* __restrict__ elem_inst,
+                                                               double* __restrict__ scale) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = e < E;
+  const int inst = ok ? __ldg(elem_inst + e) : -1;
+  const int inst0 = __shfl_sync(0xffffffffu, inst, 0);
+  const bool uniform = __all_sync(0xffffffffu, ok && inst == inst0);
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double v = ok ? fabs(means[s * E + e]) : 0.0;
+    if (!(v == v)) v = 0.0;
+    if (uniform) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if ((threadIdx.x & 31) == 0 && v > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(scale + 4 * inst0 + s), (unsigned long long)__double_as_longlong(v));
+    } else if (ok && v > 0.0) {
+      atomicMax(reinterpret_cast<unsigned long long*>(scale + 4 * inst + s), (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
 // In place allowed (V may alias out): an element reads its own coefficients
 // and only its neighbours' cell averages.
 template <int K, int P, bool AFF>
@@ -81,7 +117,9 @@ __global__ void __launch_bounds__(128) k_superbee(const nzb_mesh m, const nzb_ph
   const int64_t E = m.n_elem;
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int scaled = 0, repaired = 0;
-  if (e < E) {
+  int inst = -1;
+  if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
+  if (e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0)) {
     double u[NP][4], ub[4], sc[4];
 #pragma unroll
     for (int i = 0; i < NP; ++i)
@@ -90,7 +128,7 @@ __global__ void __launch_bounds__(128) k_superbee(const nzb_mesh m, const nzb_ph
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       ub[s] = __ldg(m.lim_means + s * E + e);
-      sc[s] = __ldg(m.lim_scale + s);
+      sc[s] = __ldg(m.lim_scale + (inst < 0 ? 0 : 4 * inst) + s);
     }
     const double share = __ldg(m.elem_share + e);
     double wsum = 0.0;

@@ -72,12 +72,13 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * elem_inst   (E)      instance of each element (null: a single instance),
  * inst_status (n_inst) nonzero = retired: its elements are left untouched,
  * inst_p_back (n_inst) back pressure of each instance (null: phys.p_back).
- * The Superbee slope limiter (physics limiter 2) needs the domain-wide maximum
- * of the cell averages, so it applies to a mesh of one instance only (no
- * elem_inst): stages and nzb_limit then run three passes after the element
- * kernel -- cell averages, their maximum, the slope limiter with the
- * positivity limiter -- and count an element as scaled when either limiter
- * changed it.
+ * The Superbee slope limiter (physics limiter 2) needs each instance's
+ * domain-wide maximum of the cell averages: stages and nzb_limit then run
+ * three passes after the element kernel -- cell averages, their maximum per
+ * instance (lim_scale holds 4 per instance: n_inst of them with elem_inst, one
+ * without), the slope limiter with the positivity limiter -- and count an
+ * element as scaled when either limiter changed it.  elem_share is each
+ * element's area over its own instance's domain area.
  * edge_pass = 1 splits every residual / stage into two launches: one thread
  * per edge evaluates each edge's fluxes once (the reference's edge_pass), then
  * the element kernel lifts them; edge_pass = 0 evaluates the fluxes inside the
@@ -113,9 +114,9 @@ typedef struct {
   double* edge_speed;       /* (n_edge) scratch of the edge pass */
   const double* elem_share; /* (E) A_e / A_domain, for the Superbee limiter (limiter 2) */
   double* lim_means;        /* (4, E) scratch of the Superbee limiter */
-  double* lim_scale;        /* (4) scratch of the Superbee limiter */
+  double* lim_scale;        /* (4 * max(1, n_inst)) scratch of the Superbee limiter */
   int32_t split;            /* threads per element of the forward kernels: 0 or 1, or 4 */
-  int32_t reserved_split;
+  int32_t n_inst;           /* instances of a batch (elem_inst values lie in [0, n_inst)); 0 or 1: one */
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly

@@ -489,6 +489,88 @@ def config4_fd(h=1e-6, tol=1e-12):
         json.dump(doc, f, indent=1)
     print("wrote config4_fd.json")
 
+class _Recorder:
+    """A reference backend behind a recording proxy: every attribute its caller reads and every method it
+    calls, with the arguments and the results (arrays stored once, by identity or equality)."""
+
+    def __init__(self, inner, log, arrays):
+        self.__dict__.update(_inner=inner, _log=log, _arrays=arrays, _ids={})
+
+    def _ref(self, v):
+        if isinstance(v, np.ndarray):
+            key = id(v)
+            if key in self._ids and np.array_equal(self._arrays[self._ids[key]], v):
+                return {"array": self._ids[key]}
+            for name, a in self._arrays.items():
+                if a.shape == v.shape and np.array_equal(a, v, equal_nan=True):
+                    self._ids[key] = name
+                    return {"array": name}
+            name = f"a{len(self._arrays)}"
+            self._arrays[name] = np.array(v, copy=True)
+            self._ids[key] = name
+            return {"array": name}
+        if isinstance(v, (tuple, list)):
+            return [self._ref(x) for x in v]
+        if isinstance(v, (np.floating, np.integer, np.bool_)):
+            return v.item()
+        return v
+
+    def __getattr__(self, name):
+        val = getattr(self._inner, name)
+        if callable(val):
+            def call(*args, **kw):
+                out = val(*args, **kw)
+                self._log.append({"call": name, "args": self._ref(list(args)), "kw": {k: self._ref(v) for k, v in kw.items()},
+                                  "out": self._ref(out)})
+                return out
+            return call
+        self._log.append({"read": name, "value": self._ref(val)})
+        return val
+
+
+def drop_in_traces():
+    """The reference's own solve_nozzle driving a recorded NumPy backend: the sequence of Backend calls
+    its march makes (asarray, run chunks, limiter_activity, to_numpy, the counters), with every argument
+    and result.  The GPU tests replay each call on the B200 backend and compare the answers."""
+    import json
+
+    import src.backends as backends
+    from src.api import build_case, solve_nozzle
+    from src.backends.numpy_backend import NumpyBackend
+
+    cases = {
+        "smooth_tri_p1_roe": dict(contour="smooth", area_ratio=2.5, element="tri", order=1, refine=0, flux="roe",
+                                  back_pressure_ratio=0.15, max_iterations=400),
+        "bell_quad_p2_hllc": dict(contour="bell", area_ratio=2.0, element="quad", order=2, refine=0, flux="hllc",
+                                  back_pressure_ratio=0.1, max_iterations=250),
+    }
+    meta, arrays = {}, {}
+    original = backends.get_backend
+    try:
+        for name, kw in cases.items():
+            log, arr = [], {}
+
+            def recorded(bname, ops, flow, opts, _log=log, _arr=arr):
+                return _Recorder(NumpyBackend(ops, flow, opts), _log, _arr)
+
+            backends.get_backend = recorded
+            kw = dict(kw)
+            max_it = kw.pop("max_iterations")
+            cs = build_case(**kw)
+            res = solve_nozzle(case=cs, cfl=0.5, tolerance=1e-10, limiter="positivity", scheme="ssprk3",
+                               max_iterations=max_it, backend="numpy", verbose=False)
+            meta[name] = {"case": {**kw, "max_iterations": max_it, "cfl": 0.5, "tolerance": 1e-10,
+                                   "limiter": "positivity", "scheme": "ssprk3"},
+                          "log": log, "iterations": int(res.iterations), "converged": bool(res.converged),
+                          "residual": float(res.residual), "message": res.message}
+            arrays.update({f"{name}/{k}": v for k, v in arr.items()})
+    finally:
+        backends.get_backend = original
+    with open(os.path.join(HERE, "drop_in_traces.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+    _save("drop_in_traces.npz", **arrays)
+
+
 if __name__ == "__main__":
     import src  # noqa: F401  -- fails loudly when the reference is not on PYTHONPATH
 
@@ -513,3 +595,5 @@ if __name__ == "__main__":
         continuation_cases()
     if "config4" in which:
         config4_fd()
+    if "dropin" in which:
+        drop_in_traces()

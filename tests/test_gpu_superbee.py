@@ -38,10 +38,37 @@ def test_superbee_ssprk3_steps_match_the_reference(cuda, kind, p):
     assert abs(res - g["run3_ssprk3_res"]) <= 1e-11 * abs(g["run3_ssprk3_res"])
 
 
-def test_superbee_is_refused_in_a_batch(cuda):
-    cfg, nz = pkg("config"), pkg("nozzle")
-    opts = cfg.SolverOptions(limiter="superbee")
-    cs = nz.build_case(element="tri", order=1, refine=0, options=opts)
-    inst = pkg("batch").Instance(cs.operators, cs.flow, opts, cs.initial_state(), cs.geometry.length)
-    with pytest.raises(NotImplementedError):
-        pkg("batch").BatchSolver([inst])
+def _superbee_cases(max_it):
+    nz, cfg = pkg("nozzle"), pkg("config")
+    opts = cfg.SolverOptions(tolerance=1e-8, max_iterations=max_it, limiter="superbee", print_interval=0)
+    spec = [("tri", 1, 0, 2.5, 0.15), ("tri", 2, 0, 1.8, 0.30), ("tri", 3, 0, 2.2, 0.10),
+            ("quad", 1, 0, 3.0, 0.20), ("quad", 2, 0, 2.5, 0.15), ("tri", 1, 1, 2.0, 0.12)]
+    out = []
+    for el, p, r, ar, pb in spec:
+        flow = cfg.FlowConditions(flux="hllc", back_pressure_ratio=pb)
+        cs = nz.build_case(element=el, order=p, refine=r, area_ratio=ar, contour="bell", flow=flow, options=opts)
+        out.append(pkg("batch").Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length, cs.geometry))
+    return out
+
+
+def test_superbee_batch_matches_one_at_a_time(cuda):
+    """Each instance of a batch is limited against its own domain (its own maximum of the cell
+    averages and area shares): the batch reproduces every one-at-a-time march, status, iteration
+    count and state.  A NaN planted on the host in one instance's initial state retires it at the
+    first check without disturbing the others (its elements stay out of the maxima and the passes)."""
+    insts = _superbee_cases(600)
+    bad = _superbee_cases(600)[0]
+    U0 = bad.U0.copy()
+    U0[3, 1, 0] = np.nan
+    bad.U0 = U0
+    solver = pkg("batch").BatchSolver(insts + [bad])
+    solver.run()
+    got = solver.results()
+    assert got[-1].status == "non-finite" and got[-1].iterations == 1
+    for inst, b in zip(insts, got):
+        bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts)
+        p = pkg("march").solve(bk, inst.U0, length=inst.length)
+        assert b.iterations == p.iterations
+        assert b.status == ("converged" if p.converged else b.status)
+        assert rel(b.U, p.U) < 1e-12
+        assert bk.n_limited > 0
