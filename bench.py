@@ -30,9 +30,16 @@ per node (density lognormal(0, 0.3), Mach U[0.2, 3] in a random direction,
 pressure lognormal(0, 0.5)), one residual per flux and one SSP-RK3 step with
 the positivity limiter; the state (320 MB) is larger than L2.
 
-Multi-GPU: design points are independent, so N GPUs run N replicas of the
-sweep (weak scaling); ``value`` = all ranks' converged solves / the slowest
-rank's time.
+``cpu_baseline`` and ``--impl reference`` time the reference's compiled CPU
+step -- its Numba backend, restated in C with OpenMP (oracle/cpu_step.c; the
+reference's Python source does not travel with this repository): seconds per
+fused SSP-RK3 iteration of one member of each (kind, order, mesh) class, times
+every point's iteration count, the points spread over every host core one
+single-threaded march each, as the reference's process-pool sweep runs them.
+
+Multi-GPU: design points are independent, so N GPUs split one sweep of 256 N
+points, 256 per GPU (weak scaling); ``value`` = all ranks' converged solves /
+the slowest rank's time.
 """
 
 from __future__ import annotations
@@ -252,61 +259,74 @@ def sweep_workload(max_iterations, n_points=SWEEP_POINTS, rank=0, world=1):
     return points, insts, index, refused
 
 
-def oracle_costs(insts, seconds):
-    """Seconds per SSP-RK3 iteration of the NumPy oracle for each (kind, order, n_elem) class of the sweep,
-    timed on a few iterations of one member of each class within a total budget of about ``seconds``."""
-    from oracle import dg_oracle as orc
-
+def _classes(insts):
     classes = {}
     for i, inst in enumerate(insts):
         classes.setdefault((inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem), i)
-    per = seconds / max(1, len(classes))
-    cost = {}
-    for key, i in classes.items():
-        inst = insts[i]
-        st = orc.Stepper(inst.ops, inst.flow, inst.opts)
-        U = np.asarray(inst.U0, float).copy()
-        U, _ = st.run(U, 1)
-        t0 = time.perf_counter()
-        n = 0
-        while n < 2 or time.perf_counter() - t0 < per:
-            U, _ = st.run(U, 1)
-            n += 1
-        cost[key] = (time.perf_counter() - t0) / n
-    return cost, len(classes)
+    return classes
 
 
-def _class_cost(args):
-    """Worker: seconds per oracle SSP-RK3 iteration on one instance, timed for about ``per`` seconds."""
-    inst, per = args
-    from oracle import dg_oracle as orc
+def _port_cost(inst, per, chunk=10):
+    """Seconds per fused SSP-RK3 iteration of the C port on one instance, one thread, timed for about
+    ``per`` seconds in chunks of ``chunk`` steps (each chunk copies the state in and out once, as the
+    reference's run() does)."""
+    from oracle import cpu_port
 
-    st = orc.Stepper(inst.ops, inst.flow, inst.opts)
-    U = np.asarray(inst.U0, float).copy()
-    U, _ = st.run(U, 1)
-    t0 = time.perf_counter()
-    n = 0
-    while n < 2 or time.perf_counter() - t0 < per:
-        U, _ = st.run(U, 1)
-        n += 1
+    cpu_port.set_threads(1)
+    st = cpu_port.CpuStepper(inst.ops, inst.flow, inst.opts)
+    U, _ = st.run(np.asarray(inst.U0, float), 1)
+    t0, n = time.perf_counter(), 0
+    while n < 2 * chunk or time.perf_counter() - t0 < per:
+        U, _ = st.run(U, chunk)
+        n += chunk
     return (time.perf_counter() - t0) / n
 
 
-def oracle_costs_parallel(insts, seconds, workers):
-    """oracle_costs with every host core busy: one class per worker process at a time (spawned), so each
+def port_costs(insts, seconds):
+    """Seconds per iteration of the C port for each (kind, order, n_elem) class of the sweep, one member
+    each, one after another on one thread, within a total of about ``seconds``."""
+    classes = _classes(insts)
+    per = seconds / max(1, len(classes))
+    return {key: _port_cost(insts[i], per) for key, i in classes.items()}, len(classes)
+
+
+def _class_cost(args):
+    """Worker: the C port's seconds per iteration on one instance (one thread), timed for about ``per`` s."""
+    inst, per = args
+    return _port_cost(inst, per)
+
+
+def port_costs_parallel(insts, seconds, workers):
+    """port_costs with every host core busy: one class per worker process at a time (spawned), so each
     per-iteration cost is measured under the contention a parallel CPU sweep would see."""
     from concurrent.futures import ProcessPoolExecutor
     import multiprocessing as mp
 
-    classes = {}
-    for i, inst in enumerate(insts):
-        classes.setdefault((inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem), i)
+    classes = _classes(insts)
     keys = list(classes)
     rounds = -(-len(keys) // workers)
     per = seconds / max(1, rounds)
     with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
         costs = list(ex.map(_class_cost, [(insts[classes[k]], per) for k in keys]))
     return dict(zip(keys, costs)), len(keys)
+
+
+def port_solve_seconds(inst, iterations, chunk=50):
+    """Wall time of one whole march on the C port: ``iterations`` steps from the initial state in chunks of
+    ``chunk`` (the march's check interval), one thread."""
+    from oracle import cpu_port
+
+    cpu_port.set_threads(1)
+    st = cpu_port.CpuStepper(inst.ops, inst.flow, inst.opts)
+    U = np.asarray(inst.U0, float)
+    t0 = time.perf_counter()
+    U, _ = st.run(U, 1)
+    done = 1
+    while done < iterations:
+        n = min(chunk, iterations - done)
+        U, _ = st.run(U, n)
+        done += n
+    return time.perf_counter() - t0
 
 
 def parallel_makespan(insts, iterations, cost, workers):
@@ -319,11 +339,6 @@ def parallel_makespan(insts, iterations, cost, workers):
         k = load.index(min(load))
         load[k] += t
     return max(load)
-
-
-def cpu_time_for(insts, iterations, cost):
-    return float(sum(it * cost[(inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem)]
-                     for inst, it in zip(insts, iterations)))
 
 
 def plain_solve(inst, torch):
@@ -627,9 +642,7 @@ def run_ours(args, rank, world, torch, dist):
         "dtype": "f64",
         "data": "synthetic: sampled operating points (seed 0) on the reference's own mesh generator and quasi-1D "
                 "initial states, built on the host",
-        "config": {"workload": f"design sweep: {args.points * world} points, {n_built_all} built, {n_refused_all} "
-                               f"refused (shock in nozzle); tri/quad p 1-3 refine 1-3, bell contour, HLLC, positivity "
-                               f"limiter, tol 1e-10, cap {args.max_iterations} iterations",
+        "config": {"workload": sweep_workload_name(args.points * world, n_built_all, n_refused_all, args.max_iterations),
                    "elements": n_elem_all, "buckets_rank0": len(solver.meshes), "outcomes": outcomes,
                    "converged_per_step": n_conv_all, "l2": "flushed (256 MB write) before each sweep",
                    "parallelism": (f"sweep of {args.points * world} points partitioned over {world} GPUs "
@@ -647,20 +660,31 @@ def run_ours(args, rank, world, torch, dist):
         line["roofline"] = mb.pop("roofline")
         line["microbench"] = mb
     if rank == 0:
-        cost, ncls = oracle_costs(insts, args.cpu_seconds)
-        t_cpu = cpu_time_for(insts, [r.iterations for r in res], cost)
+        cost, ncls = port_costs(insts, args.cpu_seconds)
+        cores = max(1, os.cpu_count() or 1)
+        t_cpu = parallel_makespan(insts, [r.iterations for r in res], cost, cores)
         line["cpu_baseline"] = {
-            "value": n_conv / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port",
-            "sample": f"NumPy oracle SSP-RK3 iterations timed on one member of each of the sweep's {ncls} "
-                      f"(kind, order, mesh) classes (~{args.cpu_seconds:.0f} s in all), scaled by every instance's "
-                      f"iteration count on the GPU; single thread"}
+            "value": n_conv / t_cpu, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"the reference's compiled CPU step (its Numba backend restated in C, oracle/cpu_step.c): "
+                      f"fused SSP-RK3 iterations timed on one member of each of the sweep's {ncls} (kind, order, "
+                      f"mesh) classes (~{args.cpu_seconds:.0f} s in all, one thread), times every point's iteration "
+                      f"count on the GPU, the points spread over {cores} cores one single-threaded march each "
+                      f"(makespan)"}
     del solver
     return line
 
 
+def sweep_workload_name(n_points, n_built, n_refused, max_iterations):
+    """The workload string both arms report, so the driver sees one configuration."""
+    return (f"design sweep: {n_points} points, {n_built} built, {n_refused} refused (shock in nozzle); tri/quad p 1-3 "
+            f"refine 1-3, bell contour, HLLC, positivity limiter, tol 1e-10, cap {max_iterations} iterations")
+
+
 def run_reference(args):
-    """The reference's CPU path on the same sweep: the NumPy oracle's per-iteration cost for each mesh class,
-    times the iteration count the reference solver itself took on each point (tests/golden/sweep_reference.json)."""
+    """The reference's CPU path on the same sweep: its compiled step (the Numba backend restated in C,
+    oracle/cpu_step.c), timed per mesh class with every host core busy, times the iteration count the
+    reference solver itself took on each point (tests/golden/sweep_reference.json), the points spread over
+    the cores one single-threaded march each; then two whole marches timed end to end to check that model."""
     path = os.path.join(GOLDEN, "sweep_reference.json")
     base = {"impl": "reference", "metric": "batched steady design-sweep solves/s at 1e-10 scaled residual (converged solves)"}
     if not os.path.exists(path):
@@ -674,24 +698,33 @@ def run_reference(args):
     workers = max(1, os.cpu_count() or 1)
     ts = []
     for _ in range(args.warmup):
-        oracle_costs_parallel(insts, 1.0, workers)
+        port_costs_parallel(insts, 0.5, workers)
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        cost, ncls = oracle_costs_parallel(insts, args.cpu_seconds / max(1, args.steps), workers)
+        cost, ncls = port_costs_parallel(insts, args.cpu_seconds / max(1, args.steps), workers)
         ts.append(time.perf_counter() - t0)
     t_cpu = parallel_makespan(insts, its, cost, workers)
     value = n_conv / t_cpu
-    sample = (f"each step times NumPy-oracle SSP-RK3 iterations on one member of each of {ncls} mesh classes, "
-              f"{workers} at a time on {workers} cores; the sweep's CPU time is the makespan of every point's "
-              f"march (that cost times the reference solver's own iteration count) spread over the {workers} cores")
+    # the model's check: the two cheapest converged points marched whole on the C port
+    key = lambda inst: (inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem)  # noqa: E731
+    conv = sorted((its[j] * cost[key(insts[j])], j) for j, k in enumerate(index) if rows[k].get("converged"))[:2]
+    check = [{"point": int(index[j]), "iterations": int(its[j]), "modeled_s": float(m),
+              "measured_s": port_solve_seconds(insts[j], its[j])} for m, j in conv]
+    sample = (f"each step times the C port of the reference's compiled step (oracle/cpu_step.c; 1.11x the time of the "
+              f"reference's own Numba backend per iteration, geometric mean over the sweep's classes, "
+              f"oracle/numba_calibration.json) on one member of each of {ncls} mesh classes, {workers} at a time on "
+              f"{workers} cores, one thread each; the sweep's CPU time is the makespan of every point's march (that "
+              f"cost times the reference solver's own iteration count) spread over the {workers} cores")
     return {
         **base, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(ts)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "the same sampled sweep (seed 0), reference outcomes from its own solver",
-        "config": {"workload": f"design sweep: {len(points)} points, {len(insts)} built, {len(refused)} refused; "
-                               f"reference converged {n_conv}"},
+        "dtype": "f64", "data": "synthetic: sampled operating points (seed 0) on the reference's own mesh generator "
+                                "and quasi-1D initial states, built on the host",
+        "config": {"workload": sweep_workload_name(len(points), len(insts), len(refused), ref["max_iterations"]),
+                   "reference_converged": n_conv, "sweep_cpu_seconds": t_cpu},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "model_check": check,
     }
 
 
@@ -707,7 +740,7 @@ def main():
     ap.add_argument("--no-micro", action="store_true")
     ap.add_argument("--adjoint-members", type=int, default=64, help="batched-gradient members (0: skip)")
     ap.add_argument("--adjoint-cap", type=int, default=100000, help="forward iteration cap of the gradient members")
-    ap.add_argument("--cpu-seconds", type=float, default=18.0)
+    ap.add_argument("--cpu-seconds", type=float, default=18.0, help="seconds of CPU-baseline class timing")
     ap.add_argument("--micro-only", action="store_true", help="run only the residual microbench (profiling)")
     ap.add_argument("--micro-nx", type=int, default=1000, help="microbench cells along x (two triangles per cell)")
     ap.add_argument("--micro-nr", type=int, default=500, help="microbench cells across")
