@@ -604,7 +604,25 @@ class BatchGradient:
                 for k, v in merged.items()}
         return P, full
 
-    def run(self, *, adjoint_tolerance=1e-8, max_iterations=100_000, check_interval=100) -> list[MemberGradient]:
+    # adjoint status of a member whose forward solve has not retired yet (the kernels skip it), and the
+    # status a running member is parked at while newly started members take their first defect
+    WAITING, PARKED = 8, 9
+
+    def run(self, *, adjoint_tolerance=1e-8, max_iterations=100_000, check_interval=100,
+            overlap: bool = True) -> list[MemberGradient]:
+        """Every member's value and gradient.
+
+        ``overlap`` starts a member's adjoint march as soon as its own forward
+        solve has converged, while the slower members' forward solves go on:
+        each round queues one forward chunk (the forward check interval) on the
+        current stream and one adjoint chunk (``check_interval`` RK4 steps) on a
+        second stream, so the two run side by side on the device; between
+        rounds the members whose forward solves retired get their seeds and
+        frozen local steps and join the adjoint march.  ``overlap=False`` runs
+        every forward solve to retirement first, then every adjoint.  A member's
+        gradient is the same, bit for bit, either way: its seed, step and march
+        depend on its own converged state only.
+        """
         from .batch import BatchSolver
 
         import time
@@ -617,58 +635,35 @@ class BatchGradient:
         def lap(name):
             torch.cuda.synchronize(dev)
             clock.append(time.perf_counter())
-            self.timings[name] = clock[-1] - clock[-2]
+            self.timings[name] = self.timings.get(name, 0.0) + clock[-1] - clock[-2]
 
         fwd = BatchSolver(self.instances, device=dev)
-        fwd.run()
-        fres = fwd.results(with_state=False)
-        lap("forward")
         if len(fwd.meshes) != 1:
             raise NotImplementedError("the members of one batch share the element kind and order")
         dm = fwd.meshes[0]
         S0 = fwd.buffers[0][1][0]
         E, NP, NV, n = dm.E, dm.np_, dm.nf, len(self.members)
-        stream = dm.stream()
-
-        # seeds dJ/dU and the explicit dJ/da, member by member (boundary integrals in torch)
-        U_all = dm.unpack(S0)
-        seed = torch.zeros_like(U_all)
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(dev)
+        spans = [(int(fwd.local[i]), int(fwd.local[i]) + cs.operators.n_elem) for i, cs in enumerate(self.cases)]
         values = [float("nan")] * n
         J_a = [None] * n
-        spans = [(int(fwd.local[i]), int(fwd.local[i]) + cs.operators.n_elem) for i, cs in enumerate(self.cases)]
-        for i, cs in enumerate(self.cases):
-            if not fres[i].converged:
-                continue
-            lo, hi = spans[i]
-            P, full = self._params(i)
-            Ui = U_all[lo:hi].clone().requires_grad_(True)
-            X = self.case.node_coords(full, xp=torch)
-            J = objective_value(ObjectiveSpace(cs.operators, cs.flow), Ui, X, self.objective, full)
-            g = torch.autograd.grad(J, [Ui] + list(P.values()), allow_unused=True)
-            seed[lo:hi] = g[0]
-            values[i] = float(J.detach())
-            J_a[i] = {k: float(gk) if gk is not None else 0.0 for k, gk in zip(P, g[1:])}
 
-        lap("seeds")
-        # every member's adjoint march in one object; failed forward solves never start
-        status = torch.tensor([0 if r.converged else 6 for r in fres], dtype=torch.int32, device=dev)
+        # the adjoint march over the forward's concatenated mesh: it reads the forward state buffer, whose
+        # slices freeze when their members retire; every member waits until its forward solve converges
+        size = 4 * NP * E
+        z = lambda: torch.zeros(size, dtype=torch.float64, device=dev)  # noqa: E731
+        seed_soa, lam, Y1, Y2, f0, f1, f2, scratch = (z() for _ in range(8))
+        wave = torch.zeros(E, dtype=torch.float64, device=dev)
+        dt = torch.zeros(E, dtype=torch.float64, device=dev)
+        dt_new = torch.zeros(E, dtype=torch.float64, device=dev)
+        status = torch.full((n,), self.WAITING, dtype=torch.int32, device=dev)
         mesh = capi.Mesh()
         C.memmove(C.byref(mesh), C.byref(dm.c), C.sizeof(capi.Mesh))
         mesh.inst_status = status.data_ptr()
         ph = fwd.phys[0]
-        size = 4 * NP * E
-        U_soa = S0
-        seed_soa = to_soa(seed)
-        z = lambda: torch.zeros(size, dtype=torch.float64, device=dev)  # noqa: E731
-        lam, Y1, Y2, f0, f1, f2, scratch = (z() for _ in range(7))
-        wave = torch.zeros(E, dtype=torch.float64, device=dev)
-        dt = torch.zeros(E, dtype=torch.float64, device=dev)
-        capi.check(lib.nzb_residual(C.byref(mesh), C.byref(ph), 0, U_soa.data_ptr(), scratch.data_ptr(),
-                                    wave.data_ptr(), stream), "nzb_residual")
-        coef = step_coefficient(self.cases[0].operators.ref.order, self.case.options.cfl, "ssprk3")
-        capi.check(lib.nzb_local_dt(C.byref(mesh), wave.data_ptr(), coef, dt.data_ptr(), stream), "nzb_local_dt")
         bf = capi.AdjointBuffers()
-        bf.U, bf.seed, bf.lam, bf.Y1, bf.Y2 = (t.data_ptr() for t in (U_soa, seed_soa, lam, Y1, Y2))
+        bf.U, bf.seed, bf.lam, bf.Y1, bf.Y2 = (t.data_ptr() for t in (S0, seed_soa, lam, Y1, Y2))
         bf.f0, bf.f1, bf.f2, bf.dt = (t.data_ptr() for t in (f0, f1, f2, dt))
         t = {"elem_norm": torch.zeros(E, dtype=torch.float64, device=dev),
              "iterations": torch.zeros(n, dtype=torch.int32, device=dev),
@@ -687,16 +682,82 @@ class BatchGradient:
         h = capi.P()
         capi.check(lib.nzb_adjoint_create(1, C.byref(mesh), C.byref(ph), C.byref(bf), offs.ctypes.data, C.byref(am),
                                           C.byref(h)), "nzb_adjoint_create")
+        coef = step_coefficient(self.cases[0].operators.ref.order, self.case.options.cfl, "ssprk3")
+        started = np.zeros(n, bool)
+        elem_inst = dm.elem_inst_t
+
+        def start(members, fst):
+            """Seeds, frozen steps and first defects of members whose forward solves have retired."""
+            conv = [i for i in members if fst[i] == 1]
+            for i in members:
+                started[i] = True
+            if not conv:
+                return
+            U_all = dm.unpack(S0)
+            seed = dm.unpack(seed_soa)
+            for i in conv:  # dJ/dU and the explicit dJ/da (boundary integrals in torch)
+                lo, hi = spans[i]
+                P, full = self._params(i)
+                Ui = U_all[lo:hi].clone().requires_grad_(True)
+                X = self.case.node_coords(full, xp=torch)
+                J = objective_value(ObjectiveSpace(self.cases[i].operators, self.cases[i].flow), Ui, X, self.objective,
+                                    full)
+                g = torch.autograd.grad(J, [Ui] + list(P.values()), allow_unused=True)
+                seed[lo:hi] = g[0]
+                values[i] = float(J.detach())
+                J_a[i] = {k: float(gk) if gk is not None else 0.0 for k, gk in zip(P, g[1:])}
+            seed_soa.copy_(to_soa(seed))
+            # the frozen local step of the new members from their converged states (the residual runs on
+            # their elements only), written into their slices of dt
+            idx = torch.as_tensor(conv, dtype=torch.int32, device=dev)
+            only = torch.ones(n, dtype=torch.int32, device=dev)
+            only[idx.long()] = 0
+            one = capi.Mesh()
+            C.memmove(C.byref(one), C.byref(mesh), C.sizeof(capi.Mesh))
+            one.inst_status = only.data_ptr()
+            capi.check(lib.nzb_residual(C.byref(one), C.byref(ph), 0, S0.data_ptr(), scratch.data_ptr(),
+                                        wave.data_ptr(), main.cuda_stream), "nzb_residual")
+            capi.check(lib.nzb_local_dt(C.byref(one), wave.data_ptr(), coef, dt_new.data_ptr(), main.cuda_stream),
+                       "nzb_local_dt")
+            new_elem = torch.isin(elem_inst, idx)
+            dt.copy_(torch.where(new_elem, dt_new, dt))
+            # first defect (res0) of the new members alone: the running ones are parked meanwhile
+            running = status == 0
+            status.copy_(torch.where(running, torch.full_like(status, self.PARKED), status))
+            status[idx.long()] = 0
+            capi.check(lib.nzb_adjoint_run(h.value, 0, main.cuda_stream), "nzb_adjoint_run")
+            status.copy_(torch.where(running, torch.zeros_like(status), status))
+
         try:
-            capi.check(lib.nzb_adjoint_run(h.value, 0, stream), "nzb_adjoint_run")
-            done = 0
-            while int(t["n_running"].item()) > 0 and done < max_iterations:
-                k = min(check_interval, max_iterations - done)
-                capi.check(lib.nzb_adjoint_run(h.value, k, stream), "nzb_adjoint_run")
-                done += k
+            fwd_running = fwd.step_chunk(1, True)
+            fchunk = min(max(1, fwd.opts.check_interval), fwd.opts.max_iterations)
+            adj_running = 0
+            while True:
+                fst = fwd.t["status"].cpu().numpy()
+                new = [i for i in range(n) if not started[i] and fst[i] != 0]
+                if new and (overlap or not fwd_running):
+                    if not overlap:
+                        lap("forward")
+                    start(new, fst)
+                    adj_running = int((status == 0).sum().item())
+                # the adjoint stream starts after this round's set-up, before the forward chunk is queued,
+                # so the two chunks run side by side
+                side.wait_stream(main)
+                if fwd_running:
+                    fwd.launch_chunk(min(fchunk, fwd.opts.max_iterations - fwd.done), False)
+                if adj_running:
+                    capi.check(lib.nzb_adjoint_run(h.value, check_interval, side.cuda_stream), "nzb_adjoint_run")
+                main.wait_stream(side)
+                if not fwd_running and not adj_running:
+                    break
+                if fwd_running:
+                    fwd_running = fwd.n_running() if fwd.done < fwd.opts.max_iterations else 0
+                if adj_running:
+                    adj_running = int(t["n_running"].item())
+            lap("adjoint" if not overlap else "forward+adjoint")
         finally:
             lib.nzb_adjoint_destroy(h.value)
-        lap("adjoint")
+        fres = fwd.results(with_state=False)
         ast = status.cpu().numpy()
         its = t["iterations"].cpu().numpy()
         rel = (t["res"] / torch.where(t["res0"] > 0, t["res0"], torch.ones_like(t["res0"]))).cpu().numpy()
@@ -711,7 +772,8 @@ class BatchGradient:
         gvert = torch.zeros(2 * NV * E, dtype=torch.float64, device=dev)
         gpb = torch.zeros(E, dtype=torch.float64, device=dev)
         dgs = np.ascontiguousarray(face_tangent_table(self.cases[0].operators.ref).ravel())
-        capi.check(lib.nzb_vjp_coords(C.byref(mesh), C.byref(ph), U_soa.data_ptr(), lam.data_ptr(), verts.data_ptr(),
+        stream = dm.stream()
+        capi.check(lib.nzb_vjp_coords(C.byref(mesh), C.byref(ph), S0.data_ptr(), lam.data_ptr(), verts.data_ptr(),
                                       dgs.ctypes.data, gvert.data_ptr(), gpb.data_ptr(), stream), "nzb_vjp_coords")
         gv = gvert.reshape(2, NV, E).cpu().numpy()
         gp = gpb.cpu().numpy()

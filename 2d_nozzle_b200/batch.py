@@ -216,12 +216,20 @@ class BatchSolver:
         bucket and step, plus the check."""
         return sum((3 if dm.order > 0 else 2) * n for dm in self.meshes) + 1
 
-    def step_chunk(self, n: int, first: bool) -> int:
+    def launch_chunk(self, n: int, first: bool) -> None:
+        """Queue one n-step chunk (and its retirement check) on the current stream; no synchronisation."""
         capi.check(self.lib.nzb_batch_run(self.handle, int(n), 1 if first else 0, self._stream), "nzb_batch_run")
         self.done += n
         self.chunks += 1
         self.launches += self.launches_per_chunk(n)
+
+    def n_running(self) -> int:
+        """Instances still marching after the last queued chunk (waits for it)."""
         return int(self.t["n_running"].item())
+
+    def step_chunk(self, n: int, first: bool) -> int:
+        self.launch_chunk(n, first)
+        return self.n_running()
 
     def reset(self) -> None:
         """Put every instance back at its initial state with a fresh march record."""

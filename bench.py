@@ -22,7 +22,10 @@ batched speed-up over the same attempted set.
 ``adjoint`` times thrust gradients w.r.t. eight Bezier wall offsets for 64
 perturbed members (AR 2.5, p = 2 triangles, refine 2, AUSM+-up, forward and
 adjoint to 1e-10): all members as one batch (forward batch, one adjoint march
-object, one coordinate-VJP launch) against every 8th member one at a time.
+object in which each member starts as soon as its own forward solve converges,
+one coordinate-VJP launch) against every 8th member one at a time; the same
+batch with the forward and adjoint phases run one after the other is timed
+beside it.
 
 ``roofline`` is measured on the residual-kernel microbenchmark: 1,000,000
 straight-sided cubic triangles (Np = 10) on the unit rectangle, states drawn
@@ -372,6 +375,14 @@ def adjoint_section(args, torch):
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
     ok = [r for r in out if r.grad is not None]
+    # the same batch with every forward solve finished before any adjoint starts (for comparison)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bg_p = ad.BatchGradient(dc, members, "thrust", names=names)
+    out_p = bg_p.run(adjoint_tolerance=1e-10, overlap=False)
+    torch.cuda.synchronize()
+    t_phased = time.perf_counter() - t0
+    same = all(a.grad == b.grad and a.adjoint_iterations == b.adjoint_iterations for a, b in zip(out, out_p))
     sub = list(range(0, len(members), args.plain_stride))
     t0 = time.perf_counter()
     plain = {}
@@ -431,6 +442,7 @@ def adjoint_section(args, torch):
             "adjoint_iterations_max": max(r.adjoint_iterations for r in out),
             "forward_iterations_max": max(r.forward_iterations for r in out),
             "max_rel_diff_batched_vs_plain": diff, "batched_phases_s": bg.timings,
+            "phased_seconds": t_phased, "phased_phases_s": bg_p.timings, "phased_equals_overlapped": same,
             "forward_status": {st: sum(r.forward_status == st for r in out) for st in {r.forward_status for r in out}},
             "forward_iteration_cap": args.adjoint_cap,
             "all_members_estimated_plain_seconds": est_all,

@@ -160,6 +160,25 @@ def test_batched_gradients_match_one_at_a_time(cuda):
             assert abs(r.grad[k] - grad[k]) <= 1e-7 * max(abs(grad[k]), 1e-8), (k, r.grad[k], grad[k])
 
 
+def test_overlapped_batch_gradients_equal_the_phased_ones(cuda):
+    """Members whose forward solves converge early start their adjoint marches while the others' forward
+    solves go on (overlap=True); every value, gradient and iteration count is the same, bit for bit, as
+    with every forward solve finished first.  The members' forward solves converge at different
+    iterations."""
+    ad = pkg("adjoint")
+    dc = ad.differentiable_case(contour="smooth", order=1, refine=0, back_pressure_ratio=0.15, tolerance=1e-11,
+                                max_iterations=9000)
+    members = [{"area_ratio": a, "throat_x": 0.1388} for a in (1.6, 2.0, 2.5, 3.2, 3.9)]
+    a = ad.BatchGradient(dc, members, "thrust").run(overlap=True)
+    b = ad.BatchGradient(dc, members, "thrust").run(overlap=False)
+    assert len({r.forward_iterations for r in a}) > 1
+    for ra, rb in zip(a, b):
+        assert (ra.forward_status, ra.forward_iterations, ra.adjoint_converged, ra.adjoint_iterations) == \
+               (rb.forward_status, rb.forward_iterations, rb.adjoint_converged, rb.adjoint_iterations)
+        assert ra.value == rb.value or (ra.value != ra.value and rb.value != rb.value)
+        assert ra.grad == rb.grad
+
+
 def test_bezier8_shape_gradient_matches_the_reference_fd(cuda):
     """Config 4: eight-offset wall, AR 2.5, p = 2 triangles, refine 2, AUSM+-up.
 
