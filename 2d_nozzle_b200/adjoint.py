@@ -35,6 +35,7 @@ from . import capi
 from . import nozzle as nz
 from .backend import B200Backend
 from .config import SolverOptions, step_coefficient
+from .autotune import choose_variant
 from .layout import DeviceMesh, face_tangent_table, physics_struct
 from .march import solve as march_solve
 from .mesh import INFLOW, OUTFLOW
@@ -62,6 +63,7 @@ class AdjointModel:
         self.ops, self.flow, self.opts = ops, flow, opts
         self.lib = capi.load()
         self.mesh = DeviceMesh(ops, device)
+        choose_variant(self.mesh)
         self.device = self.mesh.device
         self.E, self.NP, self.NV = self.mesh.E, self.mesh.np_, self.mesh.nf
         self.phys = physics_struct(flow, opts, ops.ref)
@@ -69,8 +71,10 @@ class AdjointModel:
         self.elem_nodes = np.ascontiguousarray(np.asarray(ops.topology.elem_nodes)[:, : self.NV])
         self.elem_nodes_t = torch.as_tensor(self.elem_nodes, device=self.device)
         self.X0 = torch.as_tensor(np.asarray(ops.node_coords, float), device=self.device)
-        self._partial = torch.zeros(int(self.lib.nzb_element_blocks(self.mesh.c_ref)), dtype=torch.float64,
-                                    device=self.device)
+        # per-block partial sums of the defect: room for the most blocks any variant launches (32 elements
+        # per block); slots past the launched blocks stay zero
+        self._partial = torch.zeros(max(int(self.lib.nzb_element_blocks(self.mesh.c_ref)), (self.E + 31) // 32),
+                                    dtype=torch.float64, device=self.device)
         self._other = (None, None)  # (coordinates, DeviceMesh) of the last mesh built away from X0
 
     @property
@@ -93,7 +97,10 @@ class AdjointModel:
         # the metric terms at X are rebuilt on the device (nzb_geometry); the connectivity is this mesh's
         Xd = X.detach().to(device=self.device, dtype=torch.float64)
         if self._other[0] is None or not torch.equal(self._other[0], Xd):
-            mesh = self._other[1] if self._other[1] is not None else DeviceMesh(self.ops, self.device)
+            mesh = self._other[1]
+            if mesh is None:
+                mesh = DeviceMesh(self.ops, self.device)
+                choose_variant(mesh)
             mesh.set_geometry(Xd, self.elem_nodes_t)
             self._other = (Xd.clone(), mesh)
         return self._other[1]
@@ -732,6 +739,10 @@ class BatchGradient:
             fwd_running = fwd.step_chunk(1, True)
             fchunk = min(max(1, fwd.opts.check_interval), fwd.opts.max_iterations)
             adj_running = 0
+            # forward chunks per round: as many as take about as long as one adjoint chunk, so neither
+            # stream waits long for the other at the round's end (re-measured every round)
+            per_round = 1
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             while True:
                 fst = fwd.t["status"].cpu().numpy()
                 new = [i for i in range(n) if not started[i] and fst[i] != 0]
@@ -740,13 +751,22 @@ class BatchGradient:
                         lap("forward")
                     start(new, fst)
                     adj_running = int((status == 0).sum().item())
-                # the adjoint stream starts after this round's set-up, before the forward chunk is queued,
-                # so the two chunks run side by side
+                # the adjoint stream starts after this round's set-up, before the forward chunks are queued,
+                # so the two run side by side
                 side.wait_stream(main)
+                nf = 0
                 if fwd_running:
-                    fwd.launch_chunk(min(fchunk, fwd.opts.max_iterations - fwd.done), False)
+                    ev[0].record(main)
+                    for _ in range(per_round if adj_running else 1):
+                        if fwd.done >= fwd.opts.max_iterations:
+                            break
+                        fwd.launch_chunk(min(fchunk, fwd.opts.max_iterations - fwd.done), False)
+                        nf += 1
+                    ev[1].record(main)
                 if adj_running:
+                    ev[2].record(side)
                     capi.check(lib.nzb_adjoint_run(h.value, check_interval, side.cuda_stream), "nzb_adjoint_run")
+                    ev[3].record(side)
                 main.wait_stream(side)
                 if not fwd_running and not adj_running:
                     break
@@ -754,6 +774,10 @@ class BatchGradient:
                     fwd_running = fwd.n_running() if fwd.done < fwd.opts.max_iterations else 0
                 if adj_running:
                     adj_running = int(t["n_running"].item())
+                    if nf:
+                        t_f = ev[0].elapsed_time(ev[1]) / nf
+                        t_a = ev[2].elapsed_time(ev[3])
+                        per_round = max(1, min(64, int(round(t_a / max(t_f, 1e-3)))))
             lap("adjoint" if not overlap else "forward+adjoint")
         finally:
             lib.nzb_adjoint_destroy(h.value)

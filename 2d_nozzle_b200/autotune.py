@@ -24,8 +24,9 @@ rate, local step, update, limiter) of every variant on the sampled design
 sweep's buckets of that element type and on a large unit-rectangle mesh with
 random admissible states (the residual microbenchmark's distribution), and
 keeps the variant with the least total time over those meshes.  Without the
-file the built-in :data:`DEFAULT` applies.  ``NZB_VARIANT`` in the environment
-(``t1``, ``t1_edge`` or ``split4``) forces a variant.
+file the built-in :data:`DEFAULT` applies; ``NZB_VARIANTS_FILE`` names another
+table.  ``NZB_VARIANT`` in the environment (``t1``, ``t1_edge`` or ``split4``)
+forces a variant.
 """
 
 from __future__ import annotations
@@ -50,8 +51,15 @@ DEFAULT = {("tri", 0): "t1", ("tri", 1): "t1_edge", ("tri", 2): "split4", ("tri"
            ("quad", 0): "t1", ("quad", 1): "t1_edge", ("quad", 2): "split4", ("quad", 3): "split4"}
 
 
-def load_table(path: str = TABLE_PATH) -> dict:
+def table_path() -> str:
+    """The variant table in use: ``NZB_VARIANTS_FILE`` when set (another measured table), else the one
+    beside this module."""
+    return os.environ.get("NZB_VARIANTS_FILE") or TABLE_PATH
+
+
+def load_table(path: str | None = None) -> dict:
     """(kind, order) -> variant name, from the measured table (or the default)."""
+    path = path or table_path()
     table = dict(DEFAULT)
     if os.path.exists(path):
         with open(path) as fh:
@@ -87,11 +95,83 @@ def apply_variant(mesh, name: str) -> None:
     mesh.edge_pass = v["edge_pass"]
 
 
+# The adjoint state kernel: one thread per element (``t1``) or four (``split4``),
+# chosen per (kind, order) from the same table ("vjp_choice"; NZB_VJP_VARIANT
+# forces one).
+VJP_VARIANTS = {"t1": 1, "split4": 4}
+VJP_DEFAULT = {(k, p): "t1" for k in KINDS for p in ORDERS}
+_VJP_TABLE = None
+
+
+def vjp_variant_for(kind: str, order: int) -> str:
+    forced = (os.environ.get("NZB_VJP_VARIANT") or "").strip()
+    if forced:
+        if forced not in VJP_VARIANTS:
+            raise ValueError(f"NZB_VJP_VARIANT={forced!r}: use one of {sorted(VJP_VARIANTS)}")
+        name = forced
+    else:
+        global _VJP_TABLE
+        if _VJP_TABLE is None:
+            table = dict(VJP_DEFAULT)
+            path = table_path()
+            if os.path.exists(path):
+                with open(path) as fh:
+                    for key, nm in json.load(fh).get("vjp_choice", {}).items():
+                        k, o = key.split(":")
+                        if nm not in VJP_VARIANTS:
+                            raise ValueError(f"{path}: unknown adjoint variant {nm!r} for {key}")
+                        table[(k, int(o))] = nm
+            _VJP_TABLE = table
+        name = _VJP_TABLE.get((kind, int(order)), "t1")
+    return "t1" if int(order) == 0 else name
+
+
 def choose_variant(mesh) -> str:
-    """Set ``mesh.split`` / ``mesh.edge_pass`` for its element type; returns the variant's name."""
+    """Set ``mesh.split`` / ``mesh.edge_pass`` / ``mesh.vjp_split`` for its element type; returns the forward
+    variant's name."""
     name = variant_for(mesh.kind, mesh.order)
     apply_variant(mesh, name)
+    mesh.vjp_split = VJP_VARIANTS[vjp_variant_for(mesh.kind, mesh.order)]
     return name
+
+
+def measure_vjp(mesh, phys, state, reps: int = 5) -> dict:
+    """Microseconds of one adjoint RK4 stage (the march's unit of work: the transposed product, the rate
+    and the stage update) on ``mesh`` for each adjoint variant (best of ``reps``); the mesh's own variant
+    is restored afterwards."""
+    import torch
+
+    lib = capi.load()
+    n = state.numel()
+    bufs = [torch.zeros(n, dtype=torch.float64, device=mesh.device) for _ in range(6)]
+    lam, seed, out, f0, f1, f2 = bufs
+    seed.normal_(generator=torch.Generator(device=mesh.device).manual_seed(0))
+    dt = torch.full((mesh.E,), 1e-3, dtype=torch.float64, device=mesh.device)
+    a = capi.AdjointArgs()
+    a.mode, a.stage = capi.ADJ_RK4, 1
+    a.U, a.lam, a.seed, a.out = state.data_ptr(), seed.data_ptr(), seed.data_ptr(), out.data_ptr()
+    a.lam0, a.dt, a.f0, a.f1, a.f2 = lam.data_ptr(), dt.data_ptr(), f0.data_ptr(), f1.data_ptr(), f2.data_ptr()
+    stream = torch.cuda.current_stream(mesh.device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    keep = mesh.vjp_split
+    res = {}
+    for name, threads in VJP_VARIANTS.items():
+        mesh.vjp_split = threads
+
+        def run():
+            capi.check(lib.nzb_vjp(C.byref(mesh.c), C.byref(phys), C.byref(a), stream.cuda_stream), "nzb_vjp")
+
+        run()
+        t = []
+        for _ in range(reps):
+            ev[0].record(stream)
+            run()
+            ev[1].record(stream)
+            ev[1].synchronize()
+            t.append(1e3 * ev[0].elapsed_time(ev[1]))
+        res[name] = {"rk4_stage_us": min(t)}
+    mesh.vjp_split = keep
+    return res
 
 
 def measure(mesh, phys, state, reps: int = 5, variants=None) -> dict:
@@ -214,6 +294,18 @@ def tune(device="cuda:0", rect_elements: int = 200_000, reps: int = 5) -> dict:
                     total[name] = total.get(name, 0.0) + t["total_us"]
             doc["measured"][key] = rows
             doc["choice"][key] = min(total, key=total.get)
+            # the adjoint kernel on the same sweep bucket and on the gradient members' bucket shape
+            vrows = {}
+            if (kind, order) in buckets:
+                dm, ph, U0 = buckets[(kind, order)]
+                vrows["sweep_bucket"] = {"elements": dm.E, "us": measure_vjp(dm, ph, U0, reps)}
+            vtotal = {}
+            for row in vrows.values():
+                for name, t in row["us"].items():
+                    vtotal[name] = vtotal.get(name, 0.0) + t["rk4_stage_us"]
+            doc.setdefault("vjp_measured", {})[key] = vrows
+            if vtotal:
+                doc.setdefault("vjp_choice", {})[key] = min(vtotal, key=vtotal.get)
     doc["choice"]["tri:0"] = "t1"
     doc["choice"]["quad:0"] = "t1"
     del bs

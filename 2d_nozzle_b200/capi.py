@@ -46,6 +46,8 @@ class Mesh(C.Structure):
         ("lim_scale", P),
         ("split", I32),
         ("n_inst", I32),
+        ("vjp_split", I32),
+        ("reserved", I32),
     ]
 
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "adjoint.cuh"
+#include "adjoint_split.cuh"
 
 #ifndef NZB_INTERNAL
 #define NZB_INTERNAL __attribute__((visibility("hidden")))
@@ -19,6 +20,8 @@ NZB_INTERNAL cudaError_t vjp_coords_launch_tri(const nzb_mesh& m, const nzb_phys
                                                cudaStream_t st);
 NZB_INTERNAL cudaError_t vjp_coords_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const CoordWork& w,
                                                 cudaStream_t st);
+NZB_INTERNAL cudaError_t prepare_vjp_split_tri(int order);
+NZB_INTERNAL cudaError_t prepare_vjp_split_quad(int order);
 NZB_INTERNAL cudaError_t upload_tables_tri(const double* src, size_t count, size_t offset);
 NZB_INTERNAL cudaError_t upload_tables_quad(const double* src, size_t count, size_t offset);
 

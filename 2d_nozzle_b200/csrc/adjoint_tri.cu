@@ -6,9 +6,28 @@ namespace {
 
 template <int K, int P, bool AFF>
 cudaError_t launch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
+  if constexpr (P > 0) {
+    if (m.vjp_split == SPLIT_T) {
+      const unsigned nb = (unsigned)((m.n_elem + SPLIT_EB - 1) / SPLIT_EB);
+      k_vjp_split<K, P, AFF><<<nb, SPLIT_T * 32, VjpSplitSmem<K, P>::BYTES, st>>>(m, ph, w);
+      return cudaGetLastError();
+    }
+  }
   const int64_t nb = (m.n_elem + Launch<K, P>::NT - 1) / Launch<K, P>::NT;
   k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
   return cudaGetLastError();
+}
+
+// The split kernel's dynamic shared memory can exceed the default 48 KB:
+// raise each instantiation's limit (once per device, at table upload).
+template <int K, int P, bool AFF>
+cudaError_t prepare_vjp() {
+  if constexpr (P == 0) {
+    return cudaSuccess;
+  } else {
+    return cudaFuncSetAttribute(k_vjp_split<K, P, AFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                VjpSplitSmem<K, P>::BYTES);
+  }
 }
 
 template <int K, int P>
@@ -35,6 +54,25 @@ cudaError_t vjp_coords_launch_tri(const nzb_mesh& m, const nzb_physics& ph, cons
     case 1: return launch_coords<0, 1>(m, ph, w, st);
     case 2: return launch_coords<0, 2>(m, ph, w, st);
     case 3: return launch_coords<0, 3>(m, ph, w, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t prepare_vjp_split_tri(int order) {
+  switch (order) {
+    case 0: return cudaSuccess;
+    case 1: {
+      const cudaError_t e = prepare_vjp<0, 1, true>();
+      return e != cudaSuccess ? e : prepare_vjp<0, 1, false>();
+    }
+    case 2: {
+      const cudaError_t e = prepare_vjp<0, 2, true>();
+      return e != cudaSuccess ? e : prepare_vjp<0, 2, false>();
+    }
+    case 3: {
+      const cudaError_t e = prepare_vjp<0, 3, true>();
+      return e != cudaSuccess ? e : prepare_vjp<0, 3, false>();
+    }
   }
   return cudaErrorInvalidValue;
 }

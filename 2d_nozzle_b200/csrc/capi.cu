@@ -53,6 +53,8 @@ static int check_mesh(const nzb_mesh* m) {
   if (m->affine && m->kind != NZB_TRI) return fail("affine geometry is for straight-sided triangles");
   if (m->n_elem <= 0) return fail("mesh has no elements");
   if (m->split != 0 && m->split != 1 && m->split != SPLIT_T) return fail("split must be 0, 1 or 4 threads per element");
+  if (m->vjp_split != 0 && m->vjp_split != 1 && m->vjp_split != SPLIT_T)
+    return fail("vjp_split must be 0, 1 or 4 threads per element");
   if (!m->area || !m->face_nbr || !m->face_code || !m->face_edge || !m->edge_geo)
     return fail("mesh arrays area/face_nbr/face_code/face_edge/edge_geo are required");
   if (!m->geo || (!m->affine && !m->minv))
@@ -81,9 +83,10 @@ static int64_t element_blocks(const nzb_mesh& m) {
   const int bt = (m.split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
   return (m.n_elem + bt - 1) / bt;
 }
-// Blocks of the adjoint element kernels (one thread per element).
+// Blocks of the adjoint state kernel (= defect partial slots): one thread per
+// element, or 32 elements per block with four threads per element.
 static int64_t adjoint_blocks(const nzb_mesh& m) {
-  const int bt = block_threads(m.kind, m.order);
+  const int bt = (m.vjp_split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
   return (m.n_elem + bt - 1) / bt;
 }
 
@@ -652,7 +655,9 @@ int nzb_upload_tables(int kind, int order, const double* tables, int64_t n) {
       cuda_check(upload_tables_fwd_quad(tables, (size_t)n, off), "table upload (quadrilaterals)") ||
       cuda_check(upload_tables_tri(tables, (size_t)n, off), "table upload (adjoint, triangles)") ||
       cuda_check(upload_tables_quad(tables, (size_t)n, off), "table upload (adjoint, quadrilaterals)") ||
-      cuda_check(kind == NZB_TRI ? prepare_split_tri(order) : prepare_split_quad(order), "split kernel attributes"))
+      cuda_check(kind == NZB_TRI ? prepare_split_tri(order) : prepare_split_quad(order), "split kernel attributes") ||
+      cuda_check(kind == NZB_TRI ? prepare_vjp_split_tri(order) : prepare_vjp_split_quad(order),
+                 "adjoint split kernel attributes"))
     return -1;
   int dev = 0;
   cudaGetDevice(&dev);

@@ -244,6 +244,7 @@ class DeviceMesh:
         m.edge_speed = self.edge_speed.data_ptr()
         m.edge_pass = 0
         m.split = 1
+        m.vjp_split = 1
         # Superbee limiter: each element's share of the domain's area and scratch
         if "area" in arrays:
             area = np.asarray(arrays["area"], float)
@@ -294,6 +295,17 @@ class DeviceMesh:
         if threads not in (1, 4):
             raise ValueError("split takes 1 or 4 threads per element")
         self.c.split = 4 if (threads == 4 and self.order > 0) else 1
+
+    @property
+    def vjp_split(self) -> int:
+        return int(self.c.vjp_split) if self.c.vjp_split > 1 else 1
+
+    @vjp_split.setter
+    def vjp_split(self, threads: int) -> None:
+        """Threads per element of the adjoint state kernel: 1, or 4 (orders >= 1)."""
+        if threads not in (1, 4):
+            raise ValueError("vjp_split takes 1 or 4 threads per element")
+        self.c.vjp_split = 4 if (threads == 4 and self.order > 0) else 1
 
     @property
     def edge_pass(self) -> bool:

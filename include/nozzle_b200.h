@@ -90,6 +90,10 @@ enum { NZB_OP_RESIDUAL = 0, NZB_OP_RATE = 1 };
  * projection by component, the limiter's probe points split -- and ignores
  * edge_pass; split = 0 or 1 runs one thread per element.  It agrees with the
  * one-thread kernels to round-off (a few sums associate differently).
+ * vjp_split = 4 (orders >= 1) runs the adjoint state kernel the same way:
+ * faces and volume points split over four warps, each warp gathering one
+ * component of every node in the one-thread kernel's order; it agrees with
+ * the one-thread kernel to round-off.
  */
 typedef struct {
   int32_t kind;
@@ -117,6 +121,8 @@ typedef struct {
   double* lim_scale;        /* (4 * max(1, n_inst)) scratch of the Superbee limiter */
   int32_t split;            /* threads per element of the forward kernels: 0 or 1, or 4 */
   int32_t n_inst;           /* instances of a batch (elem_inst values lie in [0, n_inst)); 0 or 1: one */
+  int32_t vjp_split;        /* threads per element of the adjoint state kernel (nzb_vjp, nzb_adjoint_*): 0 or 1, or 4 */
+  int32_t reserved;
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly

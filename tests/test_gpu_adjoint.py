@@ -26,11 +26,19 @@ def flow_for(flux, pb=0.9):
     return pkg("config").FlowConditions(flux=flux, back_pressure_ratio=pb)
 
 
+@pytest.fixture(params=["t1", "split4"])
+def vjp_variant(request, monkeypatch):
+    """The adjoint state kernel with one thread per element and with four."""
+    monkeypatch.setenv("NZB_VJP_VARIANT", request.param)
+    return request.param
+
+
 def model_for(ops, flow, general=False):
     ad = pkg("adjoint")
     m = ad.AdjointModel(ops, flow, pkg("config").SolverOptions(cfl=0.5))
     if general:
         m.mesh = pkg("layout").DeviceMesh(ops, m.device, force_general=True)
+        pkg("autotune").choose_variant(m.mesh)
     return m
 
 
@@ -46,7 +54,7 @@ def aos(m, a):
 
 @pytest.mark.parametrize("kind,p", TINY)
 @pytest.mark.parametrize("flux", FLUXES)
-def test_state_vjp_matches_complex_steps(cuda, kind, p, flux):
+def test_state_vjp_matches_complex_steps(cuda, kind, p, flux, vjp_variant):
     ops, g = tiny_ops(kind, p)
     flow = flow_for(flux)
     U = g["U"]
@@ -84,7 +92,7 @@ def test_coordinate_and_back_pressure_vjp_match_complex_steps(cuda, kind, p, flu
 
 
 @pytest.mark.parametrize("kind,p,flux", [("tri", 2, "hllc"), ("quad", 1, "roe")])
-def test_rate_and_rk4_march_match_the_oracle(cuda, kind, p, flux):
+def test_rate_and_rk4_march_match_the_oracle(cuda, kind, p, flux, vjp_variant):
     ad = pkg("adjoint")
     ops, g = tiny_ops(kind, p)
     flow = flow_for(flux)
@@ -103,6 +111,34 @@ def test_rate_and_rk4_march_match_the_oracle(cuda, kind, p, flux):
     assert rel(aos(m, lam_dev), ref) < 1e-10
     d_ref = orc.state_vjp(U, ref, ops, flow, J) - seed
     assert abs(rel_res - np.sqrt(np.mean(d_ref**2)) / np.sqrt(np.mean(seed**2))) < 1e-9
+
+
+@pytest.mark.parametrize("kind,p", [c for c in TINY if c[1] > 0])
+@pytest.mark.parametrize("flux", FLUXES)
+def test_vjp_split_agrees_with_one_thread(cuda, kind, p, flux, monkeypatch):
+    """Four threads per element against one in the adjoint state kernel: the product, the rate, the defect
+    norm and six RK4 steps of the march, on every tiny mesh, flux and geometry layout, to round-off."""
+    ad = pkg("adjoint")
+    ops, g = tiny_ops(kind, p)
+    flow = flow_for(flux)
+    U = g["U"]
+    rng = np.random.default_rng(3)
+    lam, seed = rng.standard_normal(U.shape), rng.standard_normal(U.shape)
+    for general in ((False, True) if kind == "tri" else (True,)):
+        out = {}
+        for name in ("t1", "split4"):
+            monkeypatch.setenv("NZB_VJP_VARIANT", name)
+            m = model_for(ops, flow, general)
+            assert m.mesh.vjp_split == (4 if name == "split4" else 1)
+            v = aos(m, m.vjp_state(soa(m, U), soa(m, lam)))
+            r = aos(m, m.adjoint_rate(soa(m, U), soa(m, lam), soa(m, seed)))
+            d = m.defect_rms(soa(m, U), soa(m, lam), soa(m, seed))
+            am = ad.AdjointMarch(m, soa(m, U), soa(m, seed), 0.5)
+            lam6, rr, its, _ = am.solve(tolerance=0.0, max_iterations=6, check_interval=3)
+            out[name] = (v, r, d, aos(m, lam6), rr)
+        a, b = out["t1"], out["split4"]
+        assert rel(b[0], a[0]) < 1e-13 and rel(b[1], a[1]) < 1e-13 and rel(b[3], a[3]) < 1e-12
+        assert abs(b[2] - a[2]) <= 1e-13 * a[2] and abs(b[4] - a[4]) <= 1e-12 * a[4]
 
 
 def test_residual_function_backward_is_the_kernels(cuda):
