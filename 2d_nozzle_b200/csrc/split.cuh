@@ -37,6 +37,17 @@
 
 #include "element.cuh"
 
+#ifndef NZB_MINB_SPLIT
+#define NZB_MINB_SPLIT 4
+#endif
+// NZB_SPLIT_ROLLED = 1: one copy of the volume-point and probe loops with the
+// warp's share as runtime bounds (table reads by runtime index), instead of a
+// copy per warp with compile-time addresses -- a quarter of the code, for the
+// instruction cache
+#ifndef NZB_SPLIT_ROLLED
+#define NZB_SPLIT_ROLLED 0
+#endif
+
 namespace nzb {
 
 constexpr int SPLIT_T = 4;   // threads (warps) per element
@@ -106,8 +117,10 @@ struct SplitSmem {
   static constexpr int NRM = LIFT;
   static constexpr int RED = LIFT + SPLIT_T * SPLIT_EB;
   static constexpr int SCR = FV;
-  // resident blocks per SM the shared memory allows (228 KB, 1 KB reserved per block), at most 4
-  static constexpr int BLOCKS = (228 * 1024) / (BYTES + 1024) < 4 ? (228 * 1024) / (BYTES + 1024) : 4;
+  // resident blocks per SM the shared memory allows (228 KB, 1 KB reserved per block), at most
+  // NZB_MINB_SPLIT (default 4: 128 registers per thread)
+  static constexpr int BLOCKS = (228 * 1024) / (BYTES + 1024) < NZB_MINB_SPLIT ? (228 * 1024) / (BYTES + 1024)
+                                                                                : NZB_MINB_SPLIT;
   static constexpr int MINB = BLOCKS < 1 ? 1 : BLOCKS;
   // phase A1 stages the neighbours' edge coefficients in FV
   static_assert(S::NF * S::NE * 4 <= S::NQV * 8, "FV too small to stage the neighbour coefficients");
@@ -210,6 +223,92 @@ __device__ __forceinline__ void split_volume(const double* col, double* fv, cons
   }
 }
 
+// Warp r's share [first, first + count) of n items, as SplitPlan::even.
+__device__ __forceinline__ void even_share(int n, int r, int& first, int& count) {
+  const int b = n / SPLIT_T, x = n % SPLIT_T;
+  count = b + (r < x ? 1 : 0);
+  first = r * b + (r < x ? r : x);
+}
+
+// split_volume with runtime bounds: the same arithmetic, table entries read by
+// runtime (warp-uniform) index.
+template <int K, int P, bool AFF>
+__device__ __forceinline__ void split_volume_rt(int Q0, int NQ, const double* col, double* fv, const nzb_mesh& m,
+                                                int64_t e, bool active, bool rate, double g) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NF = S::NF;
+  constexpr int CH = 4;
+  if (NQ <= 0) return;
+  const int64_t E = m.n_elem;
+  double xx = 0, xy = 0, yx = 0, yy = 0, det = 1.0;
+  double xv[NF], yv[NF];
+#pragma unroll
+  for (int v = 0; v < NF; ++v) xv[v] = yv[v] = 0.0;
+  if (active) {
+    if (AFF) {
+      xx = __ldg(m.geo + 0 * E + e);
+      xy = __ldg(m.geo + 1 * E + e);
+      yx = __ldg(m.geo + 2 * E + e);
+      yy = __ldg(m.geo + 3 * E + e);
+      det = __ldg(m.geo + 4 * E + e);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NF; ++v) {
+        xv[v] = __ldg(m.geo + v * E + e);
+        yv[v] = __ldg(m.geo + (NF + v) * E + e);
+      }
+    }
+  }
+  const double vs = AFF ? (rate ? 1.0 : -det) : -1.0;
+#pragma unroll 1
+  for (int c0 = 0; c0 < NQ; c0 += CH) {
+    const int nq = NQ - c0 < CH ? NQ - c0 : CH;
+    const int qb = Q0 + c0;
+    double uq[CH][4];
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) uq[k][s] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double ui[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) ui[s] = col[(i * 4 + s) * SPLIT_EB];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        if (k < nq) {
+          const double phi = c_tab[S::O_PHI + i * NQV + qb + k];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) uq[k][s] = fma(phi, ui[s], uq[k][s]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+      if (k < nq) {
+        const int q = qb + k;
+        const Prim pr = primitives_fast(uq[k], g);
+        const double F[4] = {pr.rho * pr.vx, pr.rho * pr.vx * pr.vx + pr.p, pr.rho * pr.vx * pr.vy, pr.rho * pr.vx * pr.H};
+        const double G[4] = {pr.rho * pr.vy, pr.rho * pr.vx * pr.vy, pr.rho * pr.vy * pr.vy + pr.p, pr.rho * pr.vy * pr.H};
+        double a00 = xx, a01 = xy, a10 = yx, a11 = yy;
+        if (!AFF) {
+          double x_xi, x_eta, y_xi, y_eta;
+          point_det<K, P>(xv, yv, q, x_xi, x_eta, y_xi, y_eta);
+          a00 = y_eta;
+          a01 = -x_eta;
+          a10 = -y_xi;
+          a11 = x_xi;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          fv[(q * 8 + s) * SPLIT_EB] = (a00 * F[s] + a01 * G[s]) * vs;
+          fv[(q * 8 + 4 + s) * SPLIT_EB] = (a10 * F[s] + a11 * G[s]) * vs;
+        }
+      }
+    }
+  }
+}
+
 // Phase C, probe share: probe points [P0, P0 + NPR) of the reference's probe
 // set (volume points, then the element's own face points with the basis of
 // its side of each face, src/spatial/limiter.py:78-95), node-major from the
@@ -290,6 +389,106 @@ __device__ __forceinline__ void split_probe(const double* col, double* scr, cons
       const double t = p1 < p2 ? p1 : p2;
       tstar = t < tstar ? t : tstar;
     }
+  }
+}
+
+// split_probe with runtime bounds: volume points and face points in separate
+// chunk loops, the same per-point arithmetic and summation order (face points
+// sum their edge nodes in increasing node index, as the node loop of
+// split_probe meets them).
+template <int K, int P>
+__device__ __forceinline__ void probe_chunk_finish(double (&w)[4][4], int npr, double* scr, const double (&ub)[4],
+                                                   double c, double e1, double eps_p, double g, double& rmin,
+                                                   double& pmin, double& tstar) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (k < npr) {
+      rmin = w[k][0] < rmin ? w[k][0] : rmin;
+      const double pp = pressure_at(w[k], g);
+      pmin = pp < pmin ? pp : pmin;
+      const double d0 = w[k][0] - ub[0], d1 = w[k][1] - ub[1], d2 = w[k][2] - ub[2], d3 = w[k][3] - ub[3];
+      const bool binds = !(c > 0.0) || pp < eps_p || !(w[k][0] > 0.0);
+      scr[(2 * k) * SPLIT_EB] = binds ? d3 * d0 - 0.5 * (d1 * d1 + d2 * d2) : 1.0;
+      scr[(2 * k + 1) * SPLIT_EB] = binds ? ub[3] * d0 + ub[0] * d3 - (ub[1] * d1 + ub[2] * d2) - e1 * d0 : 1.0;
+    }
+  }
+#pragma unroll 1
+  for (int k = 0; k < npr; ++k) {
+    const double a = scr[(2 * k) * SPLIT_EB], b = scr[(2 * k + 1) * SPLIT_EB];
+    if (a >= 0.0 && b >= 0.0) continue;
+    const double disc = b * b - 4.0 * a * c;
+    if (disc < 0.0) continue;
+    const double qq = -0.5 * (b + copysign(sqrt(disc), b));
+    const double r1 = a != 0.0 ? qq / a : 1e300, r2 = qq != 0.0 ? c / qq : 1e300;
+    const double p1 = r1 > 0.0 ? r1 : 1e300, p2 = r2 > 0.0 ? r2 : 1e300;
+    const double t = p1 < p2 ? p1 : p2;
+    tstar = t < tstar ? t : tstar;
+  }
+}
+
+template <int K, int P>
+__device__ __forceinline__ void split_probe_rt(int P0, int NPR, const double* col, double* scr, const double (&ub)[4],
+                                               int sides, double eps_p, double g, double& rmin, double& pmin,
+                                               double& tstar) {
+  using S = Shape<K, P>;
+  constexpr int NP = S::NP, NQV = S::NQV, NQF = S::NQF, NE = S::NE;
+  constexpr int CH = 4;
+  const double e1 = eps_p / (g - 1.0);
+  const double c = ub[3] * ub[0] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) - e1 * ub[0];
+  const int vend = P0 + NPR < NQV ? P0 + NPR : NQV;
+  // volume points
+#pragma unroll 1
+  for (int c0 = P0; c0 < vend; c0 += CH) {
+    asm volatile("" ::: "memory");
+    const int npr = vend - c0 < CH ? vend - c0 : CH;
+    double w[CH][4];
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w[k][s] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double ui[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) ui[s] = col[(i * 4 + s) * SPLIT_EB];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        if (k < npr) {
+          const double cf = c_tab[S::O_PHI + i * NQV + c0 + k];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) w[k][s] = fma(cf, ui[s], w[k][s]);
+        }
+      }
+    }
+    probe_chunk_finish<K, P>(w, npr, scr, ub, c, e1, eps_p, g, rmin, pmin, tstar);
+  }
+  // face points: the element's own trace, its side's basis, edge nodes in increasing node index
+  const int fbeg = P0 > NQV ? P0 : NQV;
+#pragma unroll 1
+  for (int c0 = fbeg; c0 < P0 + NPR; c0 += CH) {
+    asm volatile("" ::: "memory");
+    const int npr = P0 + NPR - c0 < CH ? P0 + NPR - c0 : CH;
+    double w[CH][4];
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) w[k][s] = 0.0;
+      if (k < npr) {
+        const int pt = c0 + k - NQV;
+        const int f = pt / NQF, q = pt - f * NQF;
+        const int side = (sides >> f) & 1;
+        const bool rev = edge_node(K, P, f, 0) > edge_node(K, P, f, NE - 1);
+#pragma unroll
+        for (int jj = 0; jj < NE; ++jj) {
+          const int j = rev ? NE - 1 - jj : jj;
+          const int n = edge_node(K, P, f, j);
+          const double cf = c_tab[S::O_PFE + ((side * S::NF + f) * NE + j) * NQF + q];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) w[k][s] = fma(cf, col[(n * 4 + s) * SPLIT_EB], w[k][s]);
+        }
+      }
+    }
+    probe_chunk_finish<K, P>(w, npr, scr, ub, c, e1, eps_p, g, rmin, pmin, tstar);
   }
 }
 
@@ -447,16 +646,28 @@ __global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
       smem[L::WAVE + f * EB + lane] = smax * len;
     } else {
       constexpr int n1 = PL::LATE;
+#if NZB_SPLIT_ROLLED
+      split_volume_rt<K, P, AFF>(NQV - n1, n1, col, smem + L::FV + lane, m, e, active, rate, g);
+#else
       if constexpr (n1 > 0) split_volume<K, P, AFF, NQV - n1, n1>(col, smem + L::FV + lane, m, e, active, rate, g);
+#endif
     }
     __syncthreads();
 
     // ---- phase A2: the other volume points, split evenly over the warps
+#if NZB_SPLIT_ROLLED
+    {
+      int q0, nq;
+      even_share(NQV - PL::LATE, r, q0, nq);
+      split_volume_rt<K, P, AFF>(q0, nq, col, smem + L::FV + lane, m, e, active, rate, g);
+    }
+#else
     for_part(r, [&](auto R) {
       constexpr SplitRanges pr = PL::even(NQV - PL::LATE);
       constexpr int q0 = pr.first[decltype(R)::value], nq = pr.count[decltype(R)::value];
       if constexpr (nq > 0) split_volume<K, P, AFF, q0, nq>(col, smem + L::FV + lane, m, e, active, rate, g);
     });
+#endif
     __syncthreads();
 
     double wave = 0.0;
@@ -669,12 +880,18 @@ __global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
     double rmin = 1e300, pmin = 1e300, tstar = 1e300;
     if (__syncthreads_or(probe)) {
       if (probe) {
+#if NZB_SPLIT_ROLLED
+        int p0, np;
+        even_share(S::NPROBE, r, p0, np);
+        split_probe_rt<K, P>(p0, np, col, smem + L::SCR + r * 8 * EB + lane, ub, sides, eps_p, g, rmin, pmin, tstar);
+#else
         for_part(r, [&](auto R) {
           constexpr SplitRanges pp = PL::even(S::NPROBE);
           constexpr int p0 = pp.first[decltype(R)::value], np = pp.count[decltype(R)::value];
           if constexpr (np > 0)
             split_probe<K, P, p0, np>(col, smem + L::SCR + r * 8 * EB + lane, ub, sides, eps_p, g, rmin, pmin, tstar);
         });
+#endif
       }
       smem[L::RED + (r * 3 + 0) * EB + lane] = rmin;
       smem[L::RED + (r * 3 + 1) * EB + lane] = pmin;
