@@ -165,6 +165,17 @@ class B200Backend:
                                      self._res.data_ptr(), self._stream), "nzb_norm")
         return float(self._host(self._res)[0])
 
+    def initial_state(self, geometry, host: bool = True):
+        """The quasi-1D initial state of this mesh (src/timestepping/initialize.py:41-102, the reference's
+        ``initial_condition="quasi1d"``), projected on the device (``nzb_initial_state``) from the node
+        coordinates, the nozzle ``geometry`` and this backend's flow: the reference-layout (E, NP, 4) host
+        array, or with ``host=False`` the device (4, NP, E) state."""
+        from .nozzle import quasi1d_table, wall_parameters
+
+        S = self.mesh.initial_state(self.phys, wall_parameters(geometry)[None], [quasi1d_table(geometry, self.flow)],
+                                    np.asarray(self.ops.node_coords, float), np.asarray(self.ops.topology.elem_nodes))
+        return self._host(self.mesh.unpack(S)) if host else S
+
     def performance(self, U, geom=None) -> dict:
         """The performance() metrics of a state (src/post/postprocess.py:193-255), integrated on the
         device; ``geom`` adds the throat-normalised coefficients and the ideal thrust."""

@@ -39,7 +39,7 @@ class Instance:
     ops: object
     flow: object
     opts: object
-    U0: np.ndarray
+    U0: np.ndarray | None  # (E, NP, 4); None: the quasi-1D initial state, projected on the device
     length: float = 1.0
     geometry: object = None  # the nozzle geometry: adds the throat-normalised observables
 
@@ -93,11 +93,38 @@ class BatchSolver:
         self.U0_soa = []  # each bucket's initial state, kept for reset()
         self.h2d_bytes = 0  # host -> device bytes of the set-up (states, geometry, connectivity)
         g_off = 0
+        # lean instances (operators built without per-element arrays) get their metric terms built on the
+        # device from the node coordinates; instances without an initial state get the quasi-1D one
+        # projected on the device
+        lean = [getattr(inst.ops, "inv_mass", None) is None for inst in instances]
+        device_init = [inst.U0 is None for inst in instances]
+        if len(set(lean)) > 1 or len(set(device_init)) > 1:
+            raise ValueError("the instances of a batch are all lean or all not, and all carry an initial state or none")
+        self.device_built = lean[0]
+        if device_init[0]:
+            from .nozzle import quasi1d_table, wall_parameters
+
+            if any(inst.geometry is None for inst in instances):
+                raise ValueError("an instance without an initial state needs its nozzle geometry")
+            walls = np.stack([wall_parameters(inst.geometry) for inst in instances])
+            q1d = [quasi1d_table(inst.geometry, inst.flow) for inst in instances]
         for key, mem in zip(self.bucket_keys, self.members):
-            parts = [host_arrays(instances[i].ops) for i in mem]
+            parts = [host_arrays(instances[i].ops, device_metrics=lean[0]) for i in mem]
             arrays = concat_arrays(parts)
             ref = instances[mem[0]].ops.ref
             dm = DeviceMesh(device=dev, arrays=arrays, ref=ref)
+            if lean[0] or device_init[0]:
+                nv = dm.nf
+                X, en, n_off = [], [], 0
+                for i in mem:
+                    Xi = np.asarray(instances[i].ops.node_coords, float)
+                    X.append(Xi)
+                    en.append(np.asarray(instances[i].ops.topology.elem_nodes)[:, :nv] + n_off)
+                    n_off += Xi.shape[0]
+                X, en = np.concatenate(X), np.ascontiguousarray(np.concatenate(en))
+            if lean[0]:
+                dm.set_geometry(X, en)
+                self.h2d_bytes += X.nbytes + en.size * 4
             flow0 = instances[mem[0]].flow
             for i in mem:
                 f = instances[i].flow
@@ -138,11 +165,16 @@ class BatchSolver:
                 dm.c.n_inst = n
             S = [dm.state() for _ in range(3)]
             dt = torch.zeros(dm.E, dtype=torch.float64, device=dev)
-            U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])
-            dm.pack(U0, S[0])
+            if device_init[0]:
+                dm.initial_state(ph, walls, q1d, X, en, elem_inst=dm.elem_inst_t, out=S[0])
+                self.h2d_bytes += dm.initial_h2d_bytes
+            else:
+                U0 = np.concatenate([np.asarray(instances[i].U0, float) for i in mem])
+                dm.pack(U0, S[0])
+                self.h2d_bytes += U0.nbytes
             self.U0_soa.append(S[0].clone())
             choose_variant(dm)
-            self.h2d_bytes += U0.nbytes + sum(a.nbytes for a in arrays.values() if isinstance(a, np.ndarray))
+            self.h2d_bytes += sum(a.nbytes for a in arrays.values() if isinstance(a, np.ndarray))
             bf = capi.Buffers()
             bf.S0, bf.S1, bf.S2 = (x.data_ptr() for x in S)
             bf.dt = dt.data_ptr()

@@ -210,6 +210,19 @@ class GeometryArgs(C.Structure):
     ]
 
 
+NZB_WALL_PARAMS = 20
+
+
+class InitialArgs(C.Structure):
+    _fields_ = [
+        ("verts", P),
+        ("wall", P),
+        ("q1d", P),
+        ("q1d_begin", P),
+        ("out", P),
+    ]
+
+
 # column of each per-instance sum of nzb_observables
 (OBS_MOM_OUT, OBS_MOM_IN, OBS_WALL_PX, OBS_MASS_IN, OBS_MASS_OUT, OBS_EXIT_LEN, OBS_EXIT_MACH, OBS_EXIT_P,
  OBS_EXIT_T, OBS_ENTROPY, OBS_AREA) = range(11)
@@ -227,6 +240,7 @@ SIGNATURES = [
     ("nzb_inverse_mass", C.c_int, [C.POINTER(Mesh), P, P, P]),
     ("nzb_observables", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(ObsArgs), P]),
     ("nzb_geometry", C.c_int, [C.POINTER(Mesh), C.POINTER(GeometryArgs), P]),
+    ("nzb_initial_state", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(InitialArgs), P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

@@ -720,6 +720,18 @@ int nzb_geometry(const nzb_mesh* mesh, const nzb_geometry_args* args, void* stre
   return cuda_check(e, "geometry launch");
 }
 
+int nzb_initial_state(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_initial_args* args, void* stream) {
+  if (check_mesh(mesh)) return -1;
+  if (!phys || !args || !args->verts || !args->wall || !args->q1d || !args->q1d_begin || !args->out)
+    return fail("initial_state: null argument");
+  if (!mesh->affine && !mesh->minv) return fail("initial_state: general geometry needs the mesh's minv");
+  if ((mesh->n_elem + 127) / 128 > 0x7fffffff) return fail("initial_state: too many elements for one launch");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const cudaError_t e = mesh->kind == NZB_TRI ? initial_launch_tri(*mesh, *phys, *args, st)
+                                              : initial_launch_quad(*mesh, *phys, *args, st);
+  return cuda_check(e, "initial state launch");
+}
+
 int nzb_inverse_mass(const nzb_mesh* mesh, const double* R, double* out, void* stream) {
   if (check_mesh(mesh)) return -1;
   if (!R || !out) return fail("inverse_mass: null argument");

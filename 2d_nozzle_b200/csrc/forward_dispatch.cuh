@@ -7,6 +7,7 @@
 
 #include "element.cuh"
 #include "geometry.cuh"
+#include "initial.cuh"
 #include "observe.cuh"
 #include "slope.cuh"
 
@@ -24,6 +25,10 @@ NZB_INTERNAL cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_ph
                                                  cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
+NZB_INTERNAL cudaError_t initial_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,
+                                            cudaStream_t st);
+NZB_INTERNAL cudaError_t initial_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,
+                                             cudaStream_t st);
 // raise the split kernels' dynamic shared-memory limit for one order (current device)
 NZB_INTERNAL cudaError_t prepare_split_tri(int order);
 NZB_INTERNAL cudaError_t prepare_split_quad(int order);

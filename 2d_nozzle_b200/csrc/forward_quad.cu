@@ -36,6 +36,18 @@ cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_physics& ph, co
   return cudaGetLastError();
 }
 
+cudaError_t initial_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a, cudaStream_t st) {
+  const unsigned nb = (unsigned)((m.n_elem + 127) / 128);
+  switch (m.order) {
+    case 0: k_initial_state<1, 0, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 1: k_initial_state<1, 1, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 2: k_initial_state<1, 2, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 3: k_initial_state<1, 3, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
   switch (m.order) {
     case 0: geometry<0>(m, a, st); break;

@@ -46,6 +46,22 @@ cudaError_t observables_launch_tri(const nzb_mesh& m, const nzb_physics& ph, con
   return cudaGetLastError();
 }
 
+cudaError_t initial_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a, cudaStream_t st) {
+  const unsigned nb = (unsigned)((m.n_elem + 127) / 128);
+  switch (m.order * 2 + (m.affine ? 1 : 0)) {
+    case 0: k_initial_state<0, 0, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 1: k_initial_state<0, 0, true><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 2: k_initial_state<0, 1, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 3: k_initial_state<0, 1, true><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 4: k_initial_state<0, 2, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 5: k_initial_state<0, 2, true><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 6: k_initial_state<0, 3, false><<<nb, 128, 0, st>>>(m, ph, a); break;
+    case 7: k_initial_state<0, 3, true><<<nb, 128, 0, st>>>(m, ph, a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st) {
   switch (m.order) {
     case 0: geometry<0>(m, a, st); break;

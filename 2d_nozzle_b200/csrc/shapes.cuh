@@ -34,10 +34,13 @@ __host__ __device__ constexpr int n_edge_nodes(int p) { return p + 1; }
 //   DGE [NV][NQV]   d(vertex shape function)/deta
 //   PFE [2][NF][NE][NQF]  the reference's face basis phi_face[side, f, i, q]
 //                   at the edge nodes i = edge_node(f, j)
+//   GV  [NV][NQV]   vertex shape functions at the volume points (the initial
+//                   state's point coordinates)
 __host__ __device__ constexpr int slot_size(int kind, int p) {
   return 3 * n_basis(kind, p) * n_qvol(kind, p) + n_basis(kind, p) * n_basis(kind, p) +
          n_edge_nodes(p) * n_qface(kind, p) + n_qface(kind, p) + n_basis(kind, p) + n_qvol(kind, p) +
-         2 * n_faces(kind) * n_qvol(kind, p) + 2 * n_faces(kind) * n_edge_nodes(p) * n_qface(kind, p);
+         2 * n_faces(kind) * n_qvol(kind, p) + 2 * n_faces(kind) * n_edge_nodes(p) * n_qface(kind, p) +
+         n_faces(kind) * n_qvol(kind, p);
 }
 __host__ __device__ constexpr int slot_offset(int kind, int p) {
   int off = 0;
@@ -69,6 +72,7 @@ struct Shape {
   static constexpr int O_DGX = O_WV + NQV;
   static constexpr int O_DGE = O_DGX + NF * NQV;
   static constexpr int O_PFE = O_DGE + NF * NQV;
+  static constexpr int O_GV = O_PFE + 2 * NF * NE * NQF;
   static constexpr int NPROBE = NQV + NF * NQF;  // limiter probe points
 };
 

@@ -53,8 +53,9 @@ def element_tables(ref) -> np.ndarray:
         raise NotImplementedError("device tables take straight-sided (Q=1) geometry")
     pf = np.asarray(ref.phi_face)  # (2, NF, NP, NQF)
     pfe = np.stack([np.stack([pf[sd, f][re.edge_node_ids(kind, p, f), :] for f in range(nf)]) for sd in range(2)])
+    gv = np.asarray(ref.geom_vol)  # (NV, NQV): vertex shape functions at the volume points
     return np.ascontiguousarray(np.concatenate([phi.ravel(), wxi.ravel(), weta.ravel(), minv.ravel(), e1d.ravel(), wf, mw,
-                                                w, dgx.ravel(), dge.ravel(), pfe.ravel()]))
+                                                w, dgx.ravel(), dge.ravel(), pfe.ravel(), gv.ravel()]))
 
 
 def lebesgue_constant(ref) -> float:
@@ -315,6 +316,43 @@ class DeviceMesh:
     def edge_pass(self, on: bool) -> None:
         """Face fluxes in a separate edge pass (True) or inside the element kernel (False)."""
         self.c.edge_pass = 1 if on else 0
+
+    def initial_state(self, phys, walls, q1d_tables, X, elem_nodes, elem_inst=None, out=None):
+        """The quasi-1D initial state projected on the device (``nzb_initial_state``,
+        src/timestepping/initialize.py:41-102), into ``out`` (a (4, NP, E) state; allocated when None).
+
+        ``walls`` (n_inst, NZB_WALL_PARAMS) and ``q1d_tables`` (one (4, n) array per instance) come from
+        ``nozzle.wall_parameters`` / ``nozzle.quasi1d_table``; ``X`` (n_node, 2) and ``elem_nodes``
+        (E, NV) give the element vertices; ``elem_inst`` maps the elements of a batch bucket to their
+        instance (None: every element is instance 0).  The mesh's metric terms must be in place (a
+        general mesh reads its inverse mass matrices).  Queued on the current stream."""
+        torch = self.torch
+        dev = self.device
+        Xd = torch.as_tensor(X, dtype=torch.float64, device=dev)
+        en = torch.as_tensor(np.ascontiguousarray(elem_nodes) if isinstance(elem_nodes, np.ndarray) else elem_nodes,
+                             device=dev).long()
+        Xe = Xd[en[:, : self.nf]]  # (E, NV, 2)
+        verts = torch.cat([Xe[:, :, 0].T, Xe[:, :, 1].T], 0).contiguous()
+        W = torch.as_tensor(np.ascontiguousarray(walls, dtype=float).reshape(-1), device=dev)
+        if W.numel() % capi.NZB_WALL_PARAMS:
+            raise ValueError("walls must be (n_inst, NZB_WALL_PARAMS)")
+        begin = np.cumsum([0] + [int(np.shape(t)[1]) for t in q1d_tables]).astype(np.int64)
+        if any(np.shape(t)[0] != 4 or np.shape(t)[1] < 2 for t in q1d_tables):
+            raise ValueError("each quasi-1D table is (4, n) with n >= 2")
+        Q = torch.as_tensor(np.concatenate([np.ascontiguousarray(t, dtype=float).ravel() for t in q1d_tables]),
+                            device=dev)
+        B = torch.as_tensor(begin, device=dev)
+        out = self.state() if out is None else out
+        m = capi.Mesh()
+        C.memmove(C.byref(m), C.byref(self.c), C.sizeof(capi.Mesh))
+        m.elem_inst = elem_inst.data_ptr() if elem_inst is not None else None
+        a = capi.InitialArgs()
+        a.verts, a.wall, a.q1d, a.q1d_begin, a.out = (t.data_ptr() for t in (verts, W, Q, B, out))
+        capi.check(capi.load().nzb_initial_state(C.byref(m), C.byref(phys), C.byref(a), self.stream()),
+                   "nzb_initial_state")
+        self._initial_inputs = (verts, W, Q, B)  # alive until the queued kernel has read them
+        self.initial_h2d_bytes = int(Xd.numel() * 8 + en.numel() * 8 + W.numel() * 8 + Q.numel() * 8 + B.numel() * 8)
+        return out
 
     def set_batch(self, elem_inst, inst_status, inst_p_back) -> None:
         """Attach the batch arrays (device tensors kept alive by the caller)."""

@@ -452,8 +452,40 @@ class ShockInNozzle(ValueError):
     """The operating point stands a normal shock in the diverging section."""
 
 
+WALL_FAMILIES = {"conical": 0, "bell": 1, "smooth": 1, "moc": 1, "bezier": 2, "bezier8": 3}
+
+
+def wall_parameters(geom: Geometry) -> np.ndarray:
+    """The numbers the device evaluates ``wall_half_height`` from (the header's NZB_WALL_PARAMS layout):
+    family, length, throat x, 1 - throat x, throat / inlet / exit half-heights, the Hermite end slopes,
+    the Bezier control heights, the difference step h = 1e-6 L and the eight bezier8 offsets -- each
+    formed as ``wall_half_height`` forms it."""
+    y_th, y_in = geom.throat_half_height, geom.inlet_half_height
+    y_ex = y_th * geom.area_ratio
+    x_th = geom.throat_x
+    span = 1.0 - x_th
+    dx_ds = span * geom.length
+    m0 = m1 = 0.0
+    if geom.contour in ("bell", "smooth", "moc"):
+        m0 = math.tan(geom.theta_initial()) * dx_ds
+        m1 = math.tan(math.radians(geom.theta_exit_deg)) * dx_ds
+    elif geom.contour == "bezier8":
+        m1 = math.tan(math.radians(geom.theta_exit_deg)) * dx_ds
+    c1 = y_th + geom.bezier_w1 * (y_ex - y_th)
+    c2 = y_th + geom.bezier_w2 * (y_ex - y_th)
+    out = [float(WALL_FAMILIES[geom.contour]), geom.length, x_th, span, y_th, y_in, y_ex, m0, m1, c1, c2,
+           1e-6 * geom.length] + [float(v) for v in geom.offsets]
+    return np.asarray(out, float)
+
+
+def quasi1d_table(geom: Geometry, flow) -> np.ndarray:
+    """(4, n): the quasi-1D solution's x, density, axial velocity and pressure, as the initial state reads it."""
+    sol = solve_quasi1d(geom, flow)
+    return np.ascontiguousarray(np.stack([sol.x, sol.density, sol.velocity, sol.pressure]).astype(float))
+
+
 def build_case(*, element="tri", order=1, refine=0, nx=14, nr=5, x_spacing="throat", cluster_strength=3.0,
-               cluster_width=0.12, flow=None, options=None, check_shock=True, **geom_kw) -> Case:
+               cluster_width=0.12, flow=None, options=None, check_shock=True, lean=False, **geom_kw) -> Case:
     """A nozzle case with the reference's defaults (src/api.py:159-210).
 
     Raises :class:`ShockInNozzle` for an operating point in the shocked band
@@ -470,5 +502,7 @@ def build_case(*, element="tri", order=1, refine=0, nx=14, nr=5, x_spacing="thro
     x_frac = x_distribution(topo.logical["nx_nodes"], nx, 2**refine, x_spacing, geom.throat_location() / geom.length,
                             cluster_strength, cluster_width)
     coords = msh.channel_coords(x_frac, r_frac, geom.wall, geom.length)
-    ops = build_operators(topo, coords, order)
+    # lean: no per-element operator arrays on the host -- the device builds the metric terms and the
+    # initial state from the node coordinates (DeviceMesh.set_geometry, nzb_initial_state)
+    ops = build_operators(topo, coords, order, lean=lean)
     return Case(geom, flow, options, topo, coords, ops, {"x_frac": x_frac, "r_frac": r_frac})

@@ -41,19 +41,25 @@ def sample_points(n=256, seed=0) -> list[Point]:
             for a, b, p, r, q in zip(ar, pb, order, refine, quad)]
 
 
-def build_instances(points, *, flux="hllc", tolerance=1e-10, max_iterations=200_000, contour="bell"):
-    """``(instances, index, refused)``: cases of the shock-free points, their point index, refused indices."""
+def build_instances(points, *, flux="hllc", tolerance=1e-10, max_iterations=200_000, contour="bell", lean=True):
+    """``(instances, index, refused)``: cases of the shock-free points, their point index, refused indices.
+
+    ``lean`` (the default) builds only what the host must -- topology, node coordinates, the quasi-1D
+    solution -- and leaves the metric terms and the projected initial state to the device
+    (``BatchSolver`` runs ``nzb_geometry`` and ``nzb_initial_state``); ``lean=False`` builds the
+    reference's full operators and initial state on the host, as its ``build_case`` does."""
     opts = SolverOptions(tolerance=tolerance, max_iterations=max_iterations, limiter="positivity", print_interval=0)
     instances, index, refused = [], [], []
     for k, pt in enumerate(points):
         flow = FlowConditions(flux=flux, back_pressure_ratio=pt.back_pressure_ratio)
         try:
             cs = build_case(element=pt.element, order=pt.order, refine=pt.refine, area_ratio=pt.area_ratio,
-                            contour=contour, flow=flow, options=opts)
+                            contour=contour, flow=flow, options=opts, lean=lean)
         except ShockInNozzle:
             refused.append(k)
             continue
-        instances.append(Instance(cs.operators, flow, opts, cs.initial_state(), cs.geometry.length, cs.geometry))
+        U0 = None if lean else cs.initial_state()
+        instances.append(Instance(cs.operators, flow, opts, U0, cs.geometry.length, cs.geometry))
         index.append(k)
     return instances, index, refused
 

@@ -253,12 +253,14 @@ SWEEP_POINTS = 256
 SWEEP_SEED = 0
 
 
-def sweep_workload(max_iterations, n_points=SWEEP_POINTS, rank=0, world=1):
+def sweep_workload(max_iterations, n_points=SWEEP_POINTS, rank=0, world=1, lean=True):
     """This rank's share of one sweep of ``n_points * world`` design points (seed 0): points rank, rank + world, ...
-    (with one rank, the whole ``n_points``-point sweep)."""
+    (with one rank, the whole ``n_points``-point sweep).  ``lean``: the cases as the GPU path builds them
+    (metric terms and initial states left to the device); otherwise with the reference's full host
+    operators and initial states (what the CPU legs run on)."""
     sweep = pkg("sweep")
     points = pkg("replicas").partition(sweep.sample_points(n_points * world, SWEEP_SEED), rank, world)
-    insts, index, refused = sweep.build_instances(points, max_iterations=max_iterations)
+    insts, index, refused = sweep.build_instances(points, max_iterations=max_iterations, lean=lean)
     return points, insts, index, refused
 
 
@@ -345,10 +347,12 @@ def parallel_makespan(insts, iterations, cost, workers):
 
 
 def plain_solve(inst, torch):
-    """One instance through the single-solve backend, state resident in HBM."""
+    """One instance through the single-solve backend, state resident in HBM (a lean instance: metric terms
+    and initial state built on the device, as the batch builds them)."""
     cfg = pkg("config")
-    bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts)
-    U0 = bk.mesh.pack(inst.U0).clone()
+    lean = getattr(inst.ops, "inv_mass", None) is None
+    bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts, device_metrics=lean)
+    U0 = (bk.initial_state(inst.geometry, host=False) if inst.U0 is None else bk.mesh.pack(inst.U0)).clone()
     scale = cfg.residual_scale(inst.flow, inst.length)
     return bk, U0, scale
 
@@ -560,11 +564,15 @@ def run_ours(args, rank, world, torch, dist):
     outcomes["refused"] = n_refused_all
 
     # end to end: set-up from host arrays, march, every state and status back
+    # end to end from the design points: the host builds each case's topology, node coordinates and
+    # quasi-1D solution (refusing the shocked points), the device its metric terms and initial state,
+    # then the march, every status and each point's performance() metrics
     e2e_t, h2d, d2h = [], 0, 0
     for k in range(2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sv = BatchSolver(insts)
+        insts_k, _, _ = pkg("sweep").build_instances(points, max_iterations=args.max_iterations)
+        sv = BatchSolver(insts_k)
         sv.run()
         out = sv.results(with_state=False)
         perf = sv.observables()
@@ -660,7 +668,8 @@ def run_ours(args, rank, world, torch, dist):
                    "parallelism": (f"sweep of {args.points * world} points partitioned over {world} GPUs "
                                    f"({args.points} each, points r::{world})" if world > 1 else "1 GPU")},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": "BatchSolver(host instances) -> run() -> results() + observables()"},
+                "path": "design points -> build_instances (host: topology, coordinates, quasi-1D) -> BatchSolver "
+                        "(device: metric terms, initial states) -> run() -> results() + observables()"},
         "plain": plain,
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
@@ -672,7 +681,13 @@ def run_ours(args, rank, world, torch, dist):
         line["roofline"] = mb.pop("roofline")
         line["microbench"] = mb
     if rank == 0:
-        cost, ncls = port_costs(insts, args.cpu_seconds)
+        # the C port runs on the reference's full operators: one full case per (kind, order, mesh) class
+        reps = {}
+        for j, inst in enumerate(insts):
+            reps.setdefault((inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem), j)
+        full, _, _ = pkg("sweep").build_instances([points[index[j]] for j in reps.values()],
+                                                  max_iterations=args.max_iterations, lean=False)
+        cost, ncls = port_costs(full, args.cpu_seconds)
         cores = max(1, os.cpu_count() or 1)
         t_cpu = parallel_makespan(insts, [r.iterations for r in res], cost, cores)
         line["cpu_baseline"] = {
@@ -703,7 +718,7 @@ def run_reference(args):
         return {**base, "unavailable": "tests/golden/sweep_reference.json (the reference's sweep outcomes) is missing"}
     with open(path) as f:
         ref = json.load(f)
-    points, insts, index, refused = sweep_workload(ref["max_iterations"], ref["n"])
+    points, insts, index, refused = sweep_workload(ref["max_iterations"], ref["n"], lean=False)
     rows = {r["point"]: r for r in ref["rows"]}
     its = [rows[k]["iterations"] for k in index]
     n_conv = sum(1 for k in index if rows[k].get("converged"))

@@ -435,6 +435,30 @@ typedef struct {
 } nzb_geometry_args;
 int nzb_geometry(const nzb_mesh* mesh, const nzb_geometry_args* args, void* stream);
 
+/* The quasi-1D initial state, L2-projected onto the basis on the device
+ * (src/timestepping/initialize.py:41-102, initial_condition = "quasi1d"): at
+ * every volume point the state interpolated linearly in x from the instance's
+ * quasi-1D solution, with vy = vx clip(y / y_w(x), 0, 1) y_w'(x), y_w the
+ * instance's wall and its slope by central differences with h = 1e-6 L; then
+ * U = M^-1 sum_q phi_q w_q det_q u_q.  mesh supplies kind, order, affine,
+ * n_elem, minv (general geometry) and, for a batch, elem_inst (instance 0
+ * without).  wall[i * NZB_WALL_PARAMS + k], per instance: family (0 conical,
+ * 1 cubic Hermite: bell / smooth / moc, 2 cubic Bezier, 3 bezier8), length,
+ * throat_x, 1 - throat_x, y_throat, y_inlet, y_exit, the Hermite end slopes
+ * tan(theta) (1 - throat_x) length at the throat and at the exit, the Bezier
+ * control heights c1, c2, h, and the eight bezier8 offsets (fractions of
+ * y_throat).  All arrays device memory. */
+#define NZB_WALL_PARAMS 20
+typedef struct {
+  const double* verts;      /* (2 NV, E): vertex x, then vertex y, of every element */
+  const double* wall;       /* (n_inst, NZB_WALL_PARAMS) */
+  const double* q1d;        /* the instances' quasi-1D solutions, concatenated: per instance its n points'
+                               x (increasing), then density, then axial velocity, then pressure */
+  const int64_t* q1d_begin; /* (n_inst + 1): first point of each instance's solution (a solution has n >= 2) */
+  double* out;              /* (4, NP, E) */
+} nzb_initial_args;
+int nzb_initial_state(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_initial_args* args, void* stream);
+
 const char* nzb_last_error(void);
 int nzb_version(void);
 

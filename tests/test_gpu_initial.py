@@ -1,0 +1,73 @@
+"""The quasi-1D initial state projected on the device (nzb_initial_state) and batches built on the device.
+
+Against the host projection (nozzle.quasi1d_initial, the restatement of
+src/timestepping/initialize.py:41-102) on every contour family, element kind
+and order; against the reference's own initial state of config 1
+(tests/golden/config1.npz); built from lean operators (metric terms from the
+node coordinates on the device) against the host-built ones; and a batch of
+lean instances against the same cases marched one at a time.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden, pkg, rel
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("tri", 0), ("tri", 1), ("tri", 2), ("tri", 3), ("quad", 1), ("quad", 2), ("quad", 3)]
+
+
+def _case(kind, p, contour, lean=False, refine=0, pb=0.15, ar=2.5):
+    nz, cfg = pkg("nozzle"), pkg("config")
+    flow = cfg.FlowConditions(flux="hllc", back_pressure_ratio=pb)
+    offs = tuple(np.random.default_rng(2).normal(0.0, 0.02, 8)) if contour == "bezier8" else (0.0,) * 8
+    return nz.build_case(element=kind, order=p, refine=refine, area_ratio=ar, contour=contour, flow=flow,
+                         offsets=offs, lean=lean)
+
+
+@pytest.mark.parametrize("kind,p", CASES)
+@pytest.mark.parametrize("contour", ["conical", "bell", "smooth", "bezier", "bezier8"])
+def test_device_initial_state_matches_the_host(cuda, kind, p, contour):
+    cs = _case(kind, p, contour)
+    bk = pkg("backend").B200Backend(cs.operators, cs.flow, cs.options)
+    U = bk.initial_state(cs.geometry)
+    assert rel(U, cs.initial_state()) < 1e-13
+    # the same from lean operators, the metric terms built on the device
+    cl = _case(kind, p, contour, lean=True)
+    bl = pkg("backend").B200Backend(cl.operators, cl.flow, cl.options, device_metrics=True)
+    assert rel(bl.initial_state(cl.geometry), cs.initial_state()) < 1e-12
+
+
+def test_device_initial_state_is_the_references(cuda):
+    """Config 1 (smooth, AR 2.5, p = 1 triangles, refine 1): the reference's own initial_state."""
+    g = golden("config1.npz")
+    nz, cfg = pkg("nozzle"), pkg("config")
+    flow = cfg.FlowConditions(flux="roe", back_pressure_ratio=0.15)
+    cs = nz.build_case(element="tri", order=1, refine=1, area_ratio=2.5, contour="smooth", flow=flow, lean=True)
+    assert np.array_equal(cs.node_coords, g["node_coords"])
+    bk = pkg("backend").B200Backend(cs.operators, flow, cs.options, device_metrics=True)
+    assert rel(bk.initial_state(cs.geometry), g["U0"]) < 1e-13
+
+
+def test_lean_batch_matches_one_at_a_time(cuda):
+    """A batch of lean instances (device-built metrics and initial states) against each case marched alone
+    on the same device-built mesh and initial state: status, iterations, state."""
+    cfg, b = pkg("config"), pkg("batch")
+    opts = cfg.SolverOptions(tolerance=1e-8, max_iterations=1500, limiter="positivity", print_interval=0)
+    spec = [("tri", 1, 0, 2.5, 0.15, "smooth"), ("quad", 2, 0, 2.0, 0.10, "bell"), ("tri", 3, 0, 1.8, 0.3, "conical"),
+            ("quad", 1, 1, 3.0, 0.12, "bell")]
+    insts = []
+    for kind, p, r, ar, pb, contour in spec:
+        cs = _case(kind, p, contour, lean=True, refine=r, pb=pb, ar=ar)
+        insts.append(b.Instance(cs.operators, cs.flow, opts, None, cs.geometry.length, cs.geometry))
+    solver = b.BatchSolver(insts)
+    assert solver.device_built
+    solver.run()
+    for inst, got in zip(insts, solver.results()):
+        bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts, device_metrics=True)
+        p = pkg("march").solve(bk, bk.initial_state(inst.geometry), length=inst.length)
+        assert got.iterations == p.iterations
+        assert rel(got.U, p.U) < 1e-12
