@@ -59,11 +59,12 @@ def from_soa(a, E, NP):
 class AdjointModel:
     """One mesh on the device, with what the transposed products need."""
 
-    def __init__(self, ops, flow, opts, device=None):
+    def __init__(self, ops, flow, opts, device=None, variants: str = "single"):
         self.ops, self.flow, self.opts = ops, flow, opts
         self.lib = capi.load()
+        self.variants = variants
         self.mesh = DeviceMesh(ops, device)
-        choose_variant(self.mesh)
+        choose_variant(self.mesh, variants)
         self.device = self.mesh.device
         self.E, self.NP, self.NV = self.mesh.E, self.mesh.np_, self.mesh.nf
         self.phys = physics_struct(flow, opts, ops.ref)
@@ -100,7 +101,7 @@ class AdjointModel:
             mesh = self._other[1]
             if mesh is None:
                 mesh = DeviceMesh(self.ops, self.device)
-                choose_variant(mesh)
+                choose_variant(mesh, self.variants)
             mesh.set_geometry(Xd, self.elem_nodes_t)
             self._other = (Xd.clone(), mesh)
         return self._other[1]
@@ -589,8 +590,11 @@ class BatchGradient:
     topology, order and solver options; they differ in design variables.
     """
 
-    def __init__(self, case: DifferentiableCase, members, objective="thrust", names=None, device=None):
+    def __init__(self, case: DifferentiableCase, members, objective="thrust", names=None, device=None,
+                 variants: str = "batch"):
         from .batch import Instance
+
+        self.variants = variants
 
         self.case = case
         self.members = [dict(m) for m in members]
@@ -644,7 +648,7 @@ class BatchGradient:
             clock.append(time.perf_counter())
             self.timings[name] = self.timings.get(name, 0.0) + clock[-1] - clock[-2]
 
-        fwd = BatchSolver(self.instances, device=dev)
+        fwd = BatchSolver(self.instances, device=dev, variants=self.variants)
         if len(fwd.meshes) != 1:
             raise NotImplementedError("the members of one batch share the element kind and order")
         dm = fwd.meshes[0]

@@ -12,21 +12,22 @@ The forward kernels come in three variants:
 
 They evaluate the same formulas and agree to round-off on a step (the
 compiler contracts multiply-adds differently in different kernels, and
-``split4`` associates a few sums differently).  Over a
-long march round-off differences grow, so the variant is fixed per (kind,
-order), never per mesh: a single solve and a batch of the same element type
-run the same kernels and give the same bits.
+``split4`` associates a few sums differently).  The adjoint state kernel has
+``t1`` and ``split4`` too.
+
+Which is fastest depends on the context, so the table has two: ``single``
+(one solve on its own mesh of a few thousand elements -- latency-bound, where
+four threads per element shorten an element's path) and ``batch`` (a bucket
+of a batch marching beside the other buckets -- throughput-bound, where one
+thread per element wastes fewer instructions).  Within a context the variant
+is fixed per (kind, order), never per mesh; a batch built with
+``variants="single"`` runs the plain solve's kernels and gives its bits.
 
 The table is ``variants.json`` beside this module, written by
-``python -m 2d_nozzle_b200.autotune --write`` on a B200: for every (kind,
-order) it times an SSP-RK3 first and second stage (the march's unit of work:
-rate, local step, update, limiter) of every variant on the sampled design
-sweep's buckets of that element type and on a large unit-rectangle mesh with
-random admissible states (the residual microbenchmark's distribution), and
-keeps the variant with the least total time over those meshes.  Without the
-file the built-in :data:`DEFAULT` applies; ``NZB_VARIANTS_FILE`` names another
-table.  ``NZB_VARIANT`` in the environment (``t1``, ``t1_edge`` or ``split4``)
-forces a variant.
+``python -m 2d_nozzle_b200.autotune --write`` on a B200 (see :func:`tune`).
+Without it the built-in defaults apply; ``NZB_VARIANTS_FILE`` names another
+table.  ``NZB_VARIANT`` / ``NZB_VJP_VARIANT`` in the environment force one
+forward / adjoint variant everywhere.
 """
 
 from __future__ import annotations
@@ -51,40 +52,57 @@ DEFAULT = {("tri", 0): "t1", ("tri", 1): "t1_edge", ("tri", 2): "split4", ("tri"
            ("quad", 0): "t1", ("quad", 1): "t1_edge", ("quad", 2): "split4", ("quad", 3): "split4"}
 
 
+CONTEXTS = ("single", "batch")
+# table keys per context: forward and adjoint variants
+_KEYS = {("single", "fwd"): "choice", ("batch", "fwd"): "batch_choice",
+         ("single", "vjp"): "vjp_choice", ("batch", "vjp"): "batch_vjp_choice"}
+
+
 def table_path() -> str:
     """The variant table in use: ``NZB_VARIANTS_FILE`` when set (another measured table), else the one
     beside this module."""
     return os.environ.get("NZB_VARIANTS_FILE") or TABLE_PATH
 
 
-def load_table(path: str | None = None) -> dict:
-    """(kind, order) -> variant name, from the measured table (or the default)."""
+def load_table(path: str | None = None, context: str = "single", which: str = "fwd") -> dict:
+    """(kind, order) -> variant name for a context, from the measured table (or the defaults).  A table
+    without the batch entries uses its single-solve ones for batches too."""
+    if context not in CONTEXTS:
+        raise ValueError(f"context {context!r}: use one of {CONTEXTS}")
     path = path or table_path()
-    table = dict(DEFAULT)
+    names = VARIANTS if which == "fwd" else VJP_VARIANTS
+    table = dict(DEFAULT if which == "fwd" else VJP_DEFAULT)
     if os.path.exists(path):
         with open(path) as fh:
             data = json.load(fh)
-        for key, name in data.get("choice", {}).items():
+        entries = data.get(_KEYS[(context, which)]) or data.get(_KEYS[("single", which)], {})
+        for key, name in entries.items():
             kind, order = key.split(":")
-            if name not in VARIANTS:
+            if name not in names:
                 raise ValueError(f"{path}: unknown variant {name!r} for {key}")
             table[(kind, int(order))] = name
     return table
 
 
-_TABLE = None
+_TABLES: dict = {}
 
 
-def variant_for(kind: str, order: int) -> str:
+def _lookup(kind: str, order: int, context: str, which: str) -> str:
+    key = (table_path(), context, which)
+    if key not in _TABLES:
+        _TABLES[key] = load_table(key[0], context, which)
+    return _TABLES[key].get((kind, int(order)), "t1")
+
+
+def variant_for(kind: str, order: int, context: str = "single") -> str:
+    """The forward variant of (kind, order) in a context: ``single`` (one solve on its own mesh: latency)
+    or ``batch`` (a bucket of a batch, its buckets side by side: throughput)."""
     forced = (os.environ.get("NZB_VARIANT") or "").strip()
     if forced:
         if forced not in VARIANTS:
             raise ValueError(f"NZB_VARIANT={forced!r}: use one of {sorted(VARIANTS)}")
         return forced
-    global _TABLE
-    if _TABLE is None:
-        _TABLE = load_table()
-    name = _TABLE.get((kind, int(order)), "t1")
+    name = _lookup(kind, order, context, "fwd")
     # four threads per element apply from p = 1 up
     return "t1" if (name == "split4" and int(order) == 0) else name
 
@@ -96,82 +114,30 @@ def apply_variant(mesh, name: str) -> None:
 
 
 # The adjoint state kernel: one thread per element (``t1``) or four (``split4``),
-# chosen per (kind, order) from the same table ("vjp_choice"; NZB_VJP_VARIANT
-# forces one).
+# chosen per (kind, order) and context from the same table; NZB_VJP_VARIANT
+# forces one.
 VJP_VARIANTS = {"t1": 1, "split4": 4}
 VJP_DEFAULT = {(k, p): "t1" for k in KINDS for p in ORDERS}
-_VJP_TABLE = None
 
 
-def vjp_variant_for(kind: str, order: int) -> str:
+def vjp_variant_for(kind: str, order: int, context: str = "single") -> str:
     forced = (os.environ.get("NZB_VJP_VARIANT") or "").strip()
     if forced:
         if forced not in VJP_VARIANTS:
             raise ValueError(f"NZB_VJP_VARIANT={forced!r}: use one of {sorted(VJP_VARIANTS)}")
         name = forced
     else:
-        global _VJP_TABLE
-        if _VJP_TABLE is None:
-            table = dict(VJP_DEFAULT)
-            path = table_path()
-            if os.path.exists(path):
-                with open(path) as fh:
-                    for key, nm in json.load(fh).get("vjp_choice", {}).items():
-                        k, o = key.split(":")
-                        if nm not in VJP_VARIANTS:
-                            raise ValueError(f"{path}: unknown adjoint variant {nm!r} for {key}")
-                        table[(k, int(o))] = nm
-            _VJP_TABLE = table
-        name = _VJP_TABLE.get((kind, int(order)), "t1")
+        name = _lookup(kind, order, context, "vjp")
     return "t1" if int(order) == 0 else name
 
 
-def choose_variant(mesh) -> str:
-    """Set ``mesh.split`` / ``mesh.edge_pass`` / ``mesh.vjp_split`` for its element type; returns the forward
-    variant's name."""
-    name = variant_for(mesh.kind, mesh.order)
+def choose_variant(mesh, context: str = "single") -> str:
+    """Set ``mesh.split`` / ``mesh.edge_pass`` / ``mesh.vjp_split`` for its element type in a context
+    (``single`` or ``batch``); returns the forward variant's name."""
+    name = variant_for(mesh.kind, mesh.order, context)
     apply_variant(mesh, name)
-    mesh.vjp_split = VJP_VARIANTS[vjp_variant_for(mesh.kind, mesh.order)]
+    mesh.vjp_split = VJP_VARIANTS[vjp_variant_for(mesh.kind, mesh.order, context)]
     return name
-
-
-def measure_vjp(mesh, phys, state, reps: int = 5) -> dict:
-    """Microseconds of one adjoint RK4 stage (the march's unit of work: the transposed product, the rate
-    and the stage update) on ``mesh`` for each adjoint variant (best of ``reps``); the mesh's own variant
-    is restored afterwards."""
-    import torch
-
-    lib = capi.load()
-    n = state.numel()
-    bufs = [torch.zeros(n, dtype=torch.float64, device=mesh.device) for _ in range(6)]
-    lam, seed, out, f0, f1, f2 = bufs
-    seed.normal_(generator=torch.Generator(device=mesh.device).manual_seed(0))
-    dt = torch.full((mesh.E,), 1e-3, dtype=torch.float64, device=mesh.device)
-    a = capi.AdjointArgs()
-    a.mode, a.stage = capi.ADJ_RK4, 1
-    a.U, a.lam, a.seed, a.out = state.data_ptr(), seed.data_ptr(), seed.data_ptr(), out.data_ptr()
-    a.lam0, a.dt, a.f0, a.f1, a.f2 = lam.data_ptr(), dt.data_ptr(), f0.data_ptr(), f1.data_ptr(), f2.data_ptr()
-    stream = torch.cuda.current_stream(mesh.device)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    keep = mesh.vjp_split
-    res = {}
-    for name, threads in VJP_VARIANTS.items():
-        mesh.vjp_split = threads
-
-        def run():
-            capi.check(lib.nzb_vjp(C.byref(mesh.c), C.byref(phys), C.byref(a), stream.cuda_stream), "nzb_vjp")
-
-        run()
-        t = []
-        for _ in range(reps):
-            ev[0].record(stream)
-            run()
-            ev[1].record(stream)
-            ev[1].synchronize()
-            t.append(1e3 * ev[0].elapsed_time(ev[1]))
-        res[name] = {"rk4_stage_us": min(t)}
-    mesh.vjp_split = keep
-    return res
 
 
 def measure(mesh, phys, state, reps: int = 5, variants=None) -> dict:
@@ -270,45 +236,144 @@ def _rectangle(kind, order, n_elem_target, device):
     return bk, state
 
 
-def tune(device="cuda:0", rect_elements: int = 200_000, reps: int = 5) -> dict:
-    """Measure every variant per (kind, order); returns the table document."""
+def _single_meshes(device, max_points: int = 256):
+    """One design-sweep instance per (kind, order, refine) on its own mesh, as a single solve runs it:
+    {(kind, order): [(backend, state), ...]} (metric terms and initial state built on the device)."""
+    from .backend import B200Backend
+    from .sweep import build_instances, sample_points
+
+    insts, _, _ = build_instances(sample_points(max_points, 0), max_iterations=10)
+    seen, out = set(), {}
+    for inst in insts:
+        key = (inst.ops.ref.kind, inst.ops.ref.order, inst.ops.n_elem)
+        if key in seen:
+            continue
+        seen.add(key)
+        bk = B200Backend(inst.ops, inst.flow, inst.opts, device=device, device_metrics=True)
+        out.setdefault(key[:2], []).append((bk, bk.initial_state(inst.geometry, host=False)))
+    return out
+
+
+def _batch_step_seconds(insts, table: dict, device, chunks: int = 3) -> float:
+    """Seconds per step of the whole batch (every bucket marching side by side) with the forward variants
+    of ``table`` ((kind, order) -> name): one warm chunk, then ``chunks`` timed chunks of the march's
+    check interval."""
+    import tempfile
+
     import torch
 
+    from .batch import BatchSolver
+
+    with tempfile.NamedTemporaryFile("w", suffix=".json", delete=False) as fh:
+        json.dump({"batch_choice": {f"{k}:{o}": v for (k, o), v in table.items()}}, fh)
+        path = fh.name
+    old = os.environ.get("NZB_VARIANTS_FILE")
+    os.environ["NZB_VARIANTS_FILE"] = path
+    try:
+        bs = BatchSolver(insts, device=device, variants="batch")
+        n = bs.opts.check_interval
+        bs.step_chunk(1, True)
+        bs.step_chunk(n, False)
+        st = torch.cuda.current_stream(device)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(st)
+        for _ in range(chunks):
+            bs.launch_chunk(n, False)
+        ev[1].record(st)
+        ev[1].synchronize()
+        t = ev[0].elapsed_time(ev[1]) * 1e-3 / (chunks * n)
+        del bs
+        return t
+    finally:
+        if old is None:
+            os.environ.pop("NZB_VARIANTS_FILE", None)
+        else:
+            os.environ["NZB_VARIANTS_FILE"] = old
+        os.unlink(path)
+
+
+def tune(device="cuda:0", reps: int = 5, grad_elements: int = 143_360) -> dict:
+    """Measure the variants per (kind, order) in both contexts; returns the table document.
+
+    * single solve (``choice``, ``vjp_choice``): one SSP-RK3 first and second stage and one adjoint RK4
+      stage of every variant on one design-sweep instance per mesh size, each on its own mesh (a plain
+      solve's latency);
+    * batch (``batch_choice``): coordinate descent over the buckets' forward variants, each candidate
+      timed as whole steps of the sampled 256-point sweep's batch (every bucket marching side by side:
+      throughput); a change is kept when it saves more than 1 %;
+    * batch adjoint (``batch_vjp_choice``): the adjoint RK4 stage on the sweep's bucket of that element
+      type and on a unit rectangle of ``grad_elements`` elements (the batched gradients' bucket size).
+    """
+    import torch
+
+    from .sweep import build_instances, sample_points
+
+    doc = {"device": torch.cuda.get_device_name(device), "reps": reps, "measured": {}, "choice": {},
+           "vjp_measured": {}, "vjp_choice": {}, "batch_measured": {}, "batch_choice": {},
+           "batch_vjp_measured": {}, "batch_vjp_choice": {}}
+    singles = _single_meshes(device)
+    for (kind, order), meshes in sorted(singles.items()):
+        if order == 0:
+            continue
+        key = f"{kind}:{order}"
+        rows, vrows, tot, vtot = [], [], {}, {}
+        for bk, st in meshes:
+            m = measure(bk.mesh, bk.phys, st, reps)
+            v = measure_vjp(bk.mesh, bk.phys, st, reps)
+            rows.append({"elements": bk.mesh.E, "us": m})
+            vrows.append({"elements": bk.mesh.E, "us": v})
+            for name, t in m.items():
+                tot[name] = tot.get(name, 0.0) + t["total_us"]
+            for name, t in v.items():
+                vtot[name] = vtot.get(name, 0.0) + t["rk4_stage_us"]
+        doc["measured"][key], doc["choice"][key] = rows, min(tot, key=tot.get)
+        doc["vjp_measured"][key], doc["vjp_choice"][key] = vrows, min(vtot, key=vtot.get)
+    del singles
+    torch.cuda.empty_cache()
+
+    insts, _, _ = build_instances(sample_points(256, 0), max_iterations=20000)
+    keys = sorted({(i.ops.ref.kind, i.ops.ref.order) for i in insts if i.ops.ref.order > 0})
+    table = {(k, o): "t1" for k in KINDS for o in ORDERS}
+    best = _batch_step_seconds(insts, table, device)
+    trials = [{"table": {f"{k}:{o}": table[(k, o)] for k, o in keys}, "us_per_step": 1e6 * best}]
+    for _ in range(2):
+        changed = False
+        for key in keys:
+            for name in VARIANTS:
+                if name == table[key]:
+                    continue
+                cand = dict(table)
+                cand[key] = name
+                t = _batch_step_seconds(insts, cand, device)
+                trials.append({"table": {f"{k}:{o}": cand[(k, o)] for k, o in keys}, "us_per_step": 1e6 * t})
+                if t < 0.99 * best:
+                    best, table, changed = t, cand, True
+        if not changed:
+            break
+    doc["batch_measured"] = {"workload": f"sampled 256-point sweep, {len(insts)} instances, whole-batch steps",
+                             "trials": trials, "best_us_per_step": 1e6 * best}
+    doc["batch_choice"] = {f"{k}:{o}": v for (k, o), v in sorted(table.items())}
+    del insts
+    torch.cuda.empty_cache()
+
     bs, buckets = _sweep_buckets(device)
-    doc = {"device": torch.cuda.get_device_name(device), "rect_elements": rect_elements, "reps": reps,
-           "measured": {}, "choice": {}}
-    for kind in KINDS:
-        for order in (1, 2, 3):
-            key = f"{kind}:{order}"
-            rows = {}
-            if (kind, order) in buckets:
-                dm, ph, U0 = buckets[(kind, order)]
-                rows["sweep_bucket"] = {"elements": dm.E, "us": measure(dm, ph, U0, reps)}
-            bk, state = _rectangle(kind, order, rect_elements, device)
-            rows["rectangle"] = {"elements": bk.mesh.E, "us": measure(bk.mesh, bk.phys, state, reps)}
-            del bk, state
-            torch.cuda.empty_cache()
-            total = {}
-            for row in rows.values():
-                for name, t in row["us"].items():
-                    total[name] = total.get(name, 0.0) + t["total_us"]
-            doc["measured"][key] = rows
-            doc["choice"][key] = min(total, key=total.get)
-            # the adjoint kernel on the same sweep bucket and on the gradient members' bucket shape
-            vrows = {}
-            if (kind, order) in buckets:
-                dm, ph, U0 = buckets[(kind, order)]
-                vrows["sweep_bucket"] = {"elements": dm.E, "us": measure_vjp(dm, ph, U0, reps)}
-            vtotal = {}
-            for row in vrows.values():
-                for name, t in row["us"].items():
-                    vtotal[name] = vtotal.get(name, 0.0) + t["rk4_stage_us"]
-            doc.setdefault("vjp_measured", {})[key] = vrows
-            if vtotal:
-                doc.setdefault("vjp_choice", {})[key] = min(vtotal, key=vtotal.get)
-    doc["choice"]["tri:0"] = "t1"
-    doc["choice"]["quad:0"] = "t1"
+    for (kind, order), (dm, ph, U0) in sorted(buckets.items()):
+        if order == 0:
+            continue
+        key = f"{kind}:{order}"
+        rows = {"sweep_bucket": {"elements": dm.E, "us": measure_vjp(dm, ph, U0, reps)}}
+        bk, state = _rectangle(kind, order, grad_elements, device)
+        rows["rectangle"] = {"elements": bk.mesh.E, "us": measure_vjp(bk.mesh, bk.phys, state, reps)}
+        del bk, state
+        vtot = {}
+        for row in rows.values():
+            for name, t in row["us"].items():
+                vtot[name] = vtot.get(name, 0.0) + t["rk4_stage_us"]
+        doc["batch_vjp_measured"][key], doc["batch_vjp_choice"][key] = rows, min(vtot, key=vtot.get)
     del bs
+    for k in KINDS:
+        for c in ("choice", "batch_choice"):
+            doc[c][f"{k}:0"] = "t1"
     return doc
 
 

@@ -33,7 +33,8 @@ from .layout import DeviceMesh, physics_struct
 class B200Backend:
     name = "b200"
 
-    def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False, device_metrics: bool = False):
+    def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False, device_metrics: bool = False,
+                 variants: str = "single"):
         import torch
 
         self.torch = torch
@@ -66,7 +67,7 @@ class B200Backend:
         self._solvers: dict[str, int] = {}
         self._obs = None
         # fused or edge-pass face fluxes, fixed per element type
-        choose_variant(self.mesh)
+        choose_variant(self.mesh, variants)
 
     def __del__(self):
         lib = getattr(self, "lib", None)

@@ -55,7 +55,10 @@ class InstanceResult:
 
 
 class BatchSolver:
-    def __init__(self, instances: list[Instance], device=None):
+    def __init__(self, instances: list[Instance], device=None, variants: str = "batch"):
+        """``variants``: the launch variants' context in the variant table -- ``batch`` (measured on
+        buckets marching side by side) or ``single`` (the one-solve choice, so a batch gives a plain
+        solve's bits)."""
         import torch
 
         if not instances:
@@ -173,7 +176,7 @@ class BatchSolver:
                 dm.pack(U0, S[0])
                 self.h2d_bytes += U0.nbytes
             self.U0_soa.append(S[0].clone())
-            choose_variant(dm)
+            choose_variant(dm, variants)
             self.h2d_bytes += sum(a.nbytes for a in arrays.values() if isinstance(a, np.ndarray))
             bf = capi.Buffers()
             bf.S0, bf.S1, bf.S2 = (x.data_ptr() for x in S)

@@ -40,12 +40,14 @@
 #ifndef NZB_MINB_SPLIT
 #define NZB_MINB_SPLIT 4
 #endif
-// NZB_SPLIT_ROLLED = 1: one copy of the volume-point and probe loops with the
-// warp's share as runtime bounds (table reads by runtime index), instead of a
-// copy per warp with compile-time addresses -- a quarter of the code, for the
-// instruction cache
+// NZB_SPLIT_ROLLED = 1 (the default): one copy of the volume-point and probe
+// loops with the warp's share as runtime bounds (table reads by runtime,
+// warp-uniform index); 0: a copy per warp with compile-time table addresses.
+// The one copy is a quarter of the code and the instruction cache holds it:
+// measured on a B200, stage 2 at 490 000 cubic triangles 1.114 -> 0.962 ms,
+// the residual at 245 000 cubic quadrilaterals 0.421 -> 0.340 ms.
 #ifndef NZB_SPLIT_ROLLED
-#define NZB_SPLIT_ROLLED 0
+#define NZB_SPLIT_ROLLED 1
 #endif
 
 namespace nzb {

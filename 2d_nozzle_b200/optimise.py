@@ -116,7 +116,7 @@ def minimize_batch(evaluate, starts, bounds, *, maximise=False, maxiter=25, ftol
 
 
 def optimise_case(case, starts, names, bounds, *, objective="thrust", maximise=True, maxiter=25, ftol=1e-10,
-                  adjoint_tolerance=1e-8, batch_sizes=None):
+                  adjoint_tolerance=1e-8, batch_sizes=None, variants="batch"):
     """Shape optimisations of a :class:`~.adjoint.DifferentiableCase` from several starting points.
 
     ``starts``: points (one value per name in ``names``); each evaluation is the
@@ -130,7 +130,7 @@ def optimise_case(case, starts, names, bounds, *, objective="thrust", maximise=T
 
     def evaluate(xs):
         members = [dict(zip(names, map(float, x))) for x in xs]
-        res = BatchGradient(case, members, objective, names).run(adjoint_tolerance=adjoint_tolerance)
+        res = BatchGradient(case, members, objective, names, variants=variants).run(adjoint_tolerance=adjoint_tolerance)
         out = []
         for r in res:
             if r.grad is None:

@@ -346,12 +346,13 @@ def parallel_makespan(insts, iterations, cost, workers):
     return max(load)
 
 
-def plain_solve(inst, torch):
+def plain_solve(inst, torch, variants="single"):
     """One instance through the single-solve backend, state resident in HBM (a lean instance: metric terms
-    and initial state built on the device, as the batch builds them)."""
+    and initial state built on the device, as the batch builds them).  ``variants``: the single-solve
+    kernels (the variant table's latency choice) or the batch's."""
     cfg = pkg("config")
     lean = getattr(inst.ops, "inv_mass", None) is None
-    bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts, device_metrics=lean)
+    bk = pkg("backend").B200Backend(inst.ops, inst.flow, inst.opts, device_metrics=lean, variants=variants)
     U0 = (bk.initial_state(inst.geometry, host=False) if inst.U0 is None else bk.mesh.pack(inst.U0)).clone()
     scale = cfg.residual_scale(inst.flow, inst.length)
     return bk, U0, scale
@@ -627,26 +628,36 @@ def run_ours(args, rank, world, torch, dist):
     first = {}
     for inst in insts:
         first.setdefault(key(inst), inst)
-    t_it = {}
-    for k, inst in first.items():
-        bk, U0, scale = plain_solve(inst, torch)
-        bk._S[0].copy_(U0)
-        bk.run_device(1)
-        bk.run_device(inst.opts.check_interval)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(10):
+    def class_costs(variants):
+        t_it = {}
+        for k, inst in first.items():
+            bk, U0, scale = plain_solve(inst, torch, variants)
+            bk._S[0].copy_(U0)
+            bk.run_device(1)
             bk.run_device(inst.opts.check_interval)
-            float(bk._res.item())
-        torch.cuda.synchronize()
-        t_it[k] = (time.perf_counter() - t0) / (10 * inst.opts.check_interval)
-        del bk
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(10):
+                bk.run_device(inst.opts.check_interval)
+                float(bk._res.item())
+            torch.cuda.synchronize()
+            t_it[k] = (time.perf_counter() - t0) / (10 * inst.opts.check_interval)
+            del bk
+        return t_it
+
+    t_it = class_costs("single")
+    t_same = class_costs("batch")
     est_all = float(sum(r.iterations * t_it[key(inst)] for inst, r in zip(insts, res)))
+    est_same = float(sum(r.iterations * t_same[key(inst)] for inst, r in zip(insts, res)))
     est_sub = float(sum(it * t_it[key(inst)] for inst, it in zip(sub, p_its)))
     plain.update({"all_instances_estimated_plain_seconds": est_all,
                   "all_instances_batched_seconds": t_rank / args.steps,
                   "speedup_all_instances": est_all / (t_rank / args.steps),
-                  "estimate_check": {"subset_estimated_seconds": est_sub, "subset_measured_seconds": float(np.sum(p_times))}})
+                  "estimate_check": {"subset_estimated_seconds": est_sub, "subset_measured_seconds": float(np.sum(p_times))},
+                  "same_kernels": {"note": "the plain path run with the batch's kernel variants instead of the "
+                                           "single-solve (latency) ones",
+                                   "all_instances_estimated_plain_seconds": est_same,
+                                   "speedup_all_instances": est_same / (t_rank / args.steps)}})
 
     line = {
         "metric": "batched steady design-sweep solves/s at 1e-10 scaled residual (converged solves)",

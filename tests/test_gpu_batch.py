@@ -35,7 +35,7 @@ def plain(inst):
 
 def test_batch_matches_one_at_a_time(cuda):
     insts = cases()
-    solver = pkg("batch").BatchSolver(insts)
+    solver = pkg("batch").BatchSolver(insts, variants="single")
     solver.run()
     got = solver.results()
     for inst, b in zip(insts, got):
@@ -84,7 +84,7 @@ def test_retired_instances_are_frozen(cuda):
     U0 = bad.U0.copy()
     U0[5, 0, 3] = np.nan
     bad.U0 = U0
-    solver = pkg("batch").BatchSolver([insts[0], bad, insts[1]])
+    solver = pkg("batch").BatchSolver([insts[0], bad, insts[1]], variants="single")
     solver.run()
     got = solver.results()
     assert got[1].status == "non-finite" and got[1].iterations == 1

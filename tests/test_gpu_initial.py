@@ -63,7 +63,7 @@ def test_lean_batch_matches_one_at_a_time(cuda):
     for kind, p, r, ar, pb, contour in spec:
         cs = _case(kind, p, contour, lean=True, refine=r, pb=pb, ar=ar)
         insts.append(b.Instance(cs.operators, cs.flow, opts, None, cs.geometry.length, cs.geometry))
-    solver = b.BatchSolver(insts)
+    solver = b.BatchSolver(insts, variants="single")
     assert solver.device_built
     solver.run()
     for inst, got in zip(insts, solver.results()):

@@ -20,7 +20,8 @@ def test_batched_runs_follow_the_one_at_a_time_runs(cuda):
     x0 = np.array([dc.default_params()[n] for n in NAMES])
     starts = [x0, np.array([2.2, 0.4, 0.8])]
     sizes = []
-    got = pkg("optimise").optimise_case(dc, starts, NAMES, BOUNDS, maxiter=3, batch_sizes=sizes)
+    got = pkg("optimise").optimise_case(dc, starts, NAMES, BOUNDS, maxiter=3, batch_sizes=sizes,
+                                          variants="single")
     assert sizes[0] == 2
     for x_start, r in zip(starts, got):
 

@@ -61,7 +61,7 @@ def test_superbee_batch_matches_one_at_a_time(cuda):
     U0 = bad.U0.copy()
     U0[3, 1, 0] = np.nan
     bad.U0 = U0
-    solver = pkg("batch").BatchSolver(insts + [bad])
+    solver = pkg("batch").BatchSolver(insts + [bad], variants="single")
     solver.run()
     got = solver.results()
     assert got[-1].status == "non-finite" and got[-1].iterations == 1

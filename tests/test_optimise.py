@@ -67,7 +67,7 @@ def test_optimise_case_batches_members_and_maps_failures(monkeypatch):
     seen = []
 
     class FakeBatch:
-        def __init__(self, case, members, objective, names):
+        def __init__(self, case, members, objective, names, variants="batch"):
             self.members, self.names = members, names
             seen.append(len(members))
 
