@@ -35,7 +35,7 @@ from . import capi
 from . import nozzle as nz
 from .backend import B200Backend
 from .config import SolverOptions, step_coefficient
-from .autotune import choose_variant
+from .autotune import choose_variant, set_struct_variant, tail_elements
 from .layout import DeviceMesh, face_tangent_table, physics_struct
 from .march import solve as march_solve
 from .mesh import INFLOW, OUTFLOW
@@ -630,9 +630,13 @@ class BatchGradient:
         second stream, so the two run side by side on the device; between
         rounds the members whose forward solves retired get their seeds and
         frozen local steps and join the adjoint march.  ``overlap=False`` runs
-        every forward solve to retirement first, then every adjoint.  A member's
-        gradient is the same, bit for bit, either way: its seed, step and march
-        depend on its own converged state only.
+        every forward solve to retirement first, then every adjoint.  With
+        ``variants="single"`` a member's gradient is the same, bit for bit,
+        either way: its seed, step and march depend on its own converged state
+        only.  In the default batch context the forward and adjoint marches
+        switch to the single-solve variants for their tails (few elements still
+        marching), at a point that depends on the whole batch, so the two
+        orders agree to round-off.
         """
         from .batch import BatchSolver
 
@@ -693,6 +697,21 @@ class BatchGradient:
         h = capi.P()
         capi.check(lib.nzb_adjoint_create(1, C.byref(mesh), C.byref(ph), C.byref(bf), offs.ctypes.data, C.byref(am),
                                           C.byref(h)), "nzb_adjoint_create")
+        # the adjoint's tail: a second march object over the same buffers with the single-solve variant,
+        # taken once the members still marching (and those that may yet start) hold few elements
+        cur = [h.value]
+        h_tail = None
+        tail_at = tail_elements() if self.variants == "batch" else 0
+        mesh_t = capi.Mesh()
+        C.memmove(C.byref(mesh_t), C.byref(mesh), C.sizeof(capi.Mesh))
+        set_struct_variant(mesh_t, dm.kind, dm.order, "single")
+        if tail_at and mesh_t.vjp_split != mesh.vjp_split:
+            ht = capi.P()
+            capi.check(lib.nzb_adjoint_create(1, C.byref(mesh_t), C.byref(ph), C.byref(bf), offs.ctypes.data,
+                                              C.byref(am), C.byref(ht)), "nzb_adjoint_create (tail)")
+            h_tail = ht.value
+        elem_count = np.asarray([hi - lo for lo, hi in spans], np.int64)
+        self.tail_switched = {"forward": None, "adjoint": None}
         coef = step_coefficient(self.cases[0].operators.ref.order, self.case.options.cfl, "ssprk3")
         started = np.zeros(n, bool)
         elem_inst = dm.elem_inst_t
@@ -736,7 +755,7 @@ class BatchGradient:
             running = status == 0
             status.copy_(torch.where(running, torch.full_like(status, self.PARKED), status))
             status[idx.long()] = 0
-            capi.check(lib.nzb_adjoint_run(h.value, 0, main.cuda_stream), "nzb_adjoint_run")
+            capi.check(lib.nzb_adjoint_run(cur[0], 0, main.cuda_stream), "nzb_adjoint_run")
             status.copy_(torch.where(running, torch.zeros_like(status), status))
 
         try:
@@ -769,15 +788,24 @@ class BatchGradient:
                     ev[1].record(main)
                 if adj_running:
                     ev[2].record(side)
-                    capi.check(lib.nzb_adjoint_run(h.value, check_interval, side.cuda_stream), "nzb_adjoint_run")
+                    capi.check(lib.nzb_adjoint_run(cur[0], check_interval, side.cuda_stream), "nzb_adjoint_run")
                     ev[3].record(side)
                 main.wait_stream(side)
                 if not fwd_running and not adj_running:
                     break
                 if fwd_running:
                     fwd_running = fwd.n_running() if fwd.done < fwd.opts.max_iterations else 0
+                    fwd._maybe_tail(fwd_running)
+                    if fwd.handle != fwd._main and self.tail_switched["forward"] is None:
+                        self.tail_switched["forward"] = fwd.done
                 if adj_running:
                     adj_running = int(t["n_running"].item())
+                    if h_tail is not None and cur[0] != h_tail and adj_running:
+                        ast_now = status.cpu().numpy()
+                        pending = fwd.t["status"].cpu().numpy() == 0
+                        if int(elem_count[(ast_now == 0) | pending].sum()) <= tail_at:
+                            cur[0] = h_tail
+                            self.tail_switched["adjoint"] = int(t["iterations"].max().item())
                     if nf:
                         t_f = ev[0].elapsed_time(ev[1]) / nf
                         t_a = ev[2].elapsed_time(ev[3])
@@ -785,6 +813,8 @@ class BatchGradient:
             lap("adjoint" if not overlap else "forward+adjoint")
         finally:
             lib.nzb_adjoint_destroy(h.value)
+            if h_tail is not None:
+                lib.nzb_adjoint_destroy(h_tail)
         fres = fwd.results(with_state=False)
         ast = status.cpu().numpy()
         its = t["iterations"].cpu().numpy()

@@ -131,6 +131,23 @@ def vjp_variant_for(kind: str, order: int, context: str = "single") -> str:
     return "t1" if int(order) == 0 else name
 
 
+def set_struct_variant(mc, kind: str, order: int, context: str) -> None:
+    """The variant fields of a copied ``capi.Mesh`` struct (``split``, ``edge_pass``, ``vjp_split``) set for
+    a context, as ``choose_variant`` sets a mesh's."""
+    v = VARIANTS[variant_for(kind, order, context)]
+    mc.split = v["split"] if order > 0 else 1
+    mc.edge_pass = 1 if v["edge_pass"] else 0
+    mc.vjp_split = VJP_VARIANTS[vjp_variant_for(kind, order, context)] if order > 0 else 1
+
+
+def tail_elements() -> int:
+    """Active elements below which a batch switches to the single-solve variants: with fewer, one thread
+    (or four) per active element no longer fills a B200 (148 SMs x 8 resident warps of 32 threads at the
+    one-thread kernels' 255 registers is 37 888), so latency, not throughput, decides.
+    ``NZB_TAIL_ELEMENTS`` overrides; 0 turns the switch off."""
+    return int(os.environ.get("NZB_TAIL_ELEMENTS", "32768"))
+
+
 def choose_variant(mesh, context: str = "single") -> str:
     """Set ``mesh.split`` / ``mesh.edge_pass`` / ``mesh.vjp_split`` for its element type in a context
     (``single`` or ``batch``); returns the forward variant's name."""

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import capi
 from .config import FLUX_IDS, SCHEMES, recommended_scheme, residual_scale, step_coefficient
-from .autotune import choose_variant
+from .autotune import choose_variant, set_struct_variant, tail_elements
 from .layout import DeviceMesh, concat_arrays, host_arrays, physics_struct
 
 STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "diverged", 4: "stalled", 5: "max_iterations"}
@@ -233,14 +233,37 @@ class BatchSolver:
         capi.check(self.lib.nzb_batch_create(nb, meshes, physs, bufs, offs.ctypes.data, facs.ctypes.data, C.byref(bm),
                                              C.byref(h)), "nzb_batch_create")
         self.handle = h.value
+        self._main = self.handle
+        # the tail: once the instances still marching hold few elements, the batch's throughput variants
+        # leave the GPU idle and an element's latency decides -- a second march object over the same
+        # buffers runs the single-solve variants from then on (no object when they are the same)
+        self.variants = variants
+        self._tail = None
+        self._tail_at = tail_elements() if variants == "batch" else 0
+        self._elem_count = np.asarray(end - begin, np.int64)
+        tail_meshes = []
+        for dm in self.meshes:
+            mc = capi.Mesh()
+            C.memmove(C.byref(mc), C.byref(dm.c), C.sizeof(capi.Mesh))
+            set_struct_variant(mc, dm.kind, dm.order, "single")
+            tail_meshes.append(mc)
+        if self._tail_at and any((a.split, a.edge_pass, a.vjp_split) != (dm.c.split, dm.c.edge_pass, dm.c.vjp_split)
+                                 for a, dm in zip(tail_meshes, self.meshes)):
+            ht = capi.P()
+            capi.check(self.lib.nzb_batch_create(nb, (capi.Mesh * nb)(*tail_meshes), physs, bufs, offs.ctypes.data,
+                                                 facs.ctypes.data, C.byref(bm), C.byref(ht)), "nzb_batch_create (tail)")
+            self._tail = ht.value
+        self.tail_switched_at = None  # iteration of the switch, if any
+        self._last_running = n
         self.done = 0
         self.chunks = 0
         self.launches = 0
         self._obs = None
 
     def __del__(self):
-        if getattr(self, "handle", None):
-            self.lib.nzb_batch_destroy(self.handle)
+        for h in (getattr(self, "_main", None), getattr(self, "_tail", None)):
+            if h:
+                self.lib.nzb_batch_destroy(h)
 
     @property
     def _stream(self):
@@ -262,12 +285,30 @@ class BatchSolver:
         """Instances still marching after the last queued chunk (waits for it)."""
         return int(self.t["n_running"].item())
 
+    def active_elements(self) -> int:
+        """Elements of the instances still marching (reads the statuses)."""
+        st = self.t["status"].cpu().numpy()
+        return int(self._elem_count[st == 0].sum())
+
+    def _maybe_tail(self, running: int) -> None:
+        if self._tail is None or self.handle == self._tail or running == self._last_running:
+            return
+        self._last_running = running
+        if running and self.active_elements() <= self._tail_at:
+            self.handle = self._tail
+            self.tail_switched_at = self.done
+
     def step_chunk(self, n: int, first: bool) -> int:
         self.launch_chunk(n, first)
-        return self.n_running()
+        running = self.n_running()
+        self._maybe_tail(running)
+        return running
 
     def reset(self) -> None:
         """Put every instance back at its initial state with a fresh march record."""
+        self.handle = self._main
+        self.tail_switched_at = None
+        self._last_running = len(self.instances)
         for (bf, S), U0 in zip(self.buffers, self.U0_soa):
             S[0].copy_(U0)
         for k in ("status", "iterations", "res0", "res", "window", "window_count", "elem_norm", "n_running"):
