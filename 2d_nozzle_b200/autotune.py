@@ -157,6 +157,44 @@ def choose_variant(mesh, context: str = "single") -> str:
     return name
 
 
+def measure_vjp(mesh, phys, state, reps: int = 5) -> dict:
+    """Microseconds of one adjoint RK4 stage (the march's unit of work: the transposed product, the rate
+    and the stage update) on ``mesh`` for each adjoint variant (best of ``reps``); the mesh's own variant
+    is restored afterwards."""
+    import torch
+
+    lib = capi.load()
+    n = state.numel()
+    lam, seed, out, f0, f1, f2 = (torch.zeros(n, dtype=torch.float64, device=mesh.device) for _ in range(6))
+    seed.normal_(generator=torch.Generator(device=mesh.device).manual_seed(0))
+    dt = torch.full((mesh.E,), 1e-3, dtype=torch.float64, device=mesh.device)
+    a = capi.AdjointArgs()
+    a.mode, a.stage = capi.ADJ_RK4, 1
+    a.U, a.lam, a.seed, a.out = state.data_ptr(), seed.data_ptr(), seed.data_ptr(), out.data_ptr()
+    a.lam0, a.dt, a.f0, a.f1, a.f2 = lam.data_ptr(), dt.data_ptr(), f0.data_ptr(), f1.data_ptr(), f2.data_ptr()
+    stream = torch.cuda.current_stream(mesh.device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    keep = mesh.vjp_split
+    res = {}
+    for name, threads in VJP_VARIANTS.items():
+        mesh.vjp_split = threads
+
+        def run():
+            capi.check(lib.nzb_vjp(C.byref(mesh.c), C.byref(phys), C.byref(a), stream.cuda_stream), "nzb_vjp")
+
+        run()
+        t = []
+        for _ in range(reps):
+            ev[0].record(stream)
+            run()
+            ev[1].record(stream)
+            ev[1].synchronize()
+            t.append(1e3 * ev[0].elapsed_time(ev[1]))
+        res[name] = {"rk4_stage_us": min(t)}
+    mesh.vjp_split = keep
+    return res
+
+
 def measure(mesh, phys, state, reps: int = 5, variants=None) -> dict:
     """Microseconds of one SSP-RK3 first and second stage on ``mesh`` for each variant.
 

@@ -157,6 +157,38 @@ def small_cases():
             _save(f"tiny_{kind}_p{p}.npz", **arrays)
 
 
+GENERIC_CASES = (("tri", 4, 1), ("tri", 5, 1), ("quad", 4, 1), ("tri", 2, 2), ("tri", 3, 2), ("quad", 2, 2))
+
+
+def generic_cases():
+    """The tiny-mesh fixtures for orders above 3 and curved (Q = 2) elements, as small_cases makes them."""
+    from src.api import build_case
+    from src.backends import get_backend
+    from src.config import SolverOptions
+    from src.spatial import limiter as lim
+
+    for kind, p, q in GENERIC_CASES:
+        cs = build_case(contour="smooth", element=kind, order=p, refine=0, geometry_order=q)
+        ops = cs.operators
+        U = random_state(ops.n_elem, ops.ref.n_basis)
+        # the operators' smaller arrays (the folded per-element ones follow from these)
+        arrays = {k: v for k, v in operator_arrays(cs).items() if k not in ("grad_x_m", "grad_y_m", "face_basis_m")}
+        arrays["U"] = U
+        arrays.update(per_flux(cs, U))
+        arrays.update({k + "_backflow": v for k, v in per_flux(cs, U, ("roe",), backflow=True).items()})
+        Ubad = U.copy()
+        Ubad[3, 0, 0] = -0.5
+        Ubad[7, 1, 3] = -1.0
+        Ubad[11, :, 0] = -5.0
+        arrays["U_bad"] = Ubad
+        arrays["limited_bad"] = lim.positivity_limiter(Ubad, ops, cs.flow)
+        bk = get_backend("numpy", ops, cs.flow, SolverOptions(limiter="positivity", scheme="ssprk3"))
+        V, res = bk.run(U.copy(), 3, "ssprk3")
+        arrays["run3_ssprk3"] = np.asarray(V)
+        arrays["run3_ssprk3_res"] = np.float64(res)
+        _save(f"tiny_{kind}_p{p}_q{q}.npz", **arrays)
+
+
 def superbee_cases():
     """The Superbee TVB slope limiter on a rough state of every tiny mesh, and three SSP-RK3 steps with it."""
     from src.api import build_case
@@ -597,3 +629,5 @@ if __name__ == "__main__":
         config4_fd()
     if "dropin" in which:
         drop_in_traces()
+    if "generic" in which:
+        generic_cases()

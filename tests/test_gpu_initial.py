@@ -28,17 +28,25 @@ def _case(kind, p, contour, lean=False, refine=0, pb=0.15, ar=2.5):
                          offsets=offs, lean=lean)
 
 
+# The reference's transverse velocity uses the wall's slope by a finite difference with h = 1e-6 L,
+# which amplifies a last-place difference of the wall by about 1e6.  The Hermite and straight families
+# are evaluated here in the host's operation order and agree to the bit; the Bezier families' integer
+# powers are rounded once on the device while the host's libm pow is not correctly rounded in about 5 %
+# of cases (measured), so their slopes -- and the small transverse momentum -- agree to ~1e-11.
+TOL = {"conical": 1e-13, "bell": 1e-13, "smooth": 1e-13, "bezier": 1e-10, "bezier8": 1e-10}
+
+
 @pytest.mark.parametrize("kind,p", CASES)
 @pytest.mark.parametrize("contour", ["conical", "bell", "smooth", "bezier", "bezier8"])
 def test_device_initial_state_matches_the_host(cuda, kind, p, contour):
     cs = _case(kind, p, contour)
     bk = pkg("backend").B200Backend(cs.operators, cs.flow, cs.options)
     U = bk.initial_state(cs.geometry)
-    assert rel(U, cs.initial_state()) < 1e-13
+    assert rel(U, cs.initial_state()) < TOL[contour]
     # the same from lean operators, the metric terms built on the device
     cl = _case(kind, p, contour, lean=True)
     bl = pkg("backend").B200Backend(cl.operators, cl.flow, cl.options, device_metrics=True)
-    assert rel(bl.initial_state(cl.geometry), cs.initial_state()) < 1e-12
+    assert rel(bl.initial_state(cl.geometry), cs.initial_state()) < max(TOL[contour], 1e-12)
 
 
 def test_device_initial_state_is_the_references(cuda):
