@@ -1,5 +1,9 @@
 """The drop-in backend: the reference's ``Backend`` interface on the B200 kernels.
 
+Straight elements of order 0..3 run the specialised kernels here; other meshes
+(orders above 3, curved elements) get :class:`~.generic.GenericB200Backend`
+from the same constructor.
+
 ``B200Backend(ops, flow, opts)`` has the constructor, attributes and methods of
 the reference's ``Backend`` (src/backends/base.py:81-201) -- ``residual``,
 ``inverse_mass``, ``limit``, ``time_step``, ``norm``, ``rate``,
@@ -32,6 +36,15 @@ from .layout import DeviceMesh, physics_struct
 
 class B200Backend:
     name = "b200"
+
+    def __new__(cls, ops, flow, opts, **kw):
+        # orders above 3 and curved elements run the kernels on the reference's per-element operators
+        if cls is B200Backend:
+            from .generic import GenericB200Backend, needs_generic
+
+            if needs_generic(ops):
+                return super().__new__(GenericB200Backend)
+        return super().__new__(cls)
 
     def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False, device_metrics: bool = False,
                  variants: str = "single"):

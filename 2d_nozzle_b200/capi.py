@@ -210,6 +210,19 @@ class GeometryArgs(C.Structure):
     ]
 
 
+class GenMesh(C.Structure):
+    _fields_ = [("np", I32), ("nqv", I32), ("nqf", I32), ("nface", I32), ("n_elem", I64), ("n_int", I64),
+                ("n_bnd", I64)] + [(n, P) for n in (
+                    "phi_vol", "phi_face", "w_face", "grad_x", "grad_y", "grad_x_m", "grad_y_m", "face_basis_m",
+                    "face_edge", "face_side", "face_sign", "edge_elem", "edge_face", "edge_tag", "edge_normal",
+                    "edge_jac", "edge_length", "elem_area", "mean_weights")]
+
+
+class GenUpdateArgs(C.Structure):
+    _fields_ = [("stage", I32), ("pad", I32), ("dt_factor", C.c_double), ("a", C.c_double), ("b", C.c_double)] + [
+        (n, P) for n in ("V", "U0", "F", "wave", "dt", "out", "partial")]
+
+
 NZB_WALL_PARAMS = 20
 
 
@@ -241,6 +254,10 @@ SIGNATURES = [
     ("nzb_observables", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(ObsArgs), P]),
     ("nzb_geometry", C.c_int, [C.POINTER(Mesh), C.POINTER(GeometryArgs), P]),
     ("nzb_initial_state", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(InitialArgs), P]),
+    ("nzb_gen_rate", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.c_int, P, P, P, P, P, P]),
+    ("nzb_gen_limit", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), P, P, P]),
+    ("nzb_gen_update", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.POINTER(GenUpdateArgs), P]),
+    ("nzb_gen_blocks", I64, [C.POINTER(GenMesh)]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

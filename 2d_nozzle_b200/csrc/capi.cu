@@ -720,6 +720,48 @@ int nzb_geometry(const nzb_mesh* mesh, const nzb_geometry_args* args, void* stre
   return cuda_check(e, "geometry launch");
 }
 
+// ---- any order, curved elements (generic.cuh)
+static int check_gen(const nzb_gen_mesh* m, const nzb_physics* ph) {
+  if (!m || !ph) return fail("generic: null mesh or physics");
+  if (m->np < 1 || m->np > 36 || m->nqv < 1 || m->nqf < 1 || (m->nface != 3 && m->nface != 4))
+    return fail("generic: sizes out of range (NP 1..36, 3 or 4 faces)");
+  if (m->n_elem < 1 || m->n_int < 0 || m->n_bnd < 0 || (m->n_elem + 127) / 128 > 0x7fffffff ||
+      (m->n_int + m->n_bnd + 127) / 128 > 0x7fffffff)
+    return fail("generic: bad element or edge count");
+  if (!m->phi_vol || !m->phi_face || !m->w_face || !m->face_edge || !m->face_side || !m->face_sign || !m->edge_elem ||
+      !m->edge_face || (m->n_bnd && !m->edge_tag) || !m->edge_normal || !m->edge_jac || !m->edge_length)
+    return fail("generic: missing mesh array");
+  return 0;
+}
+
+int64_t nzb_gen_blocks(const nzb_gen_mesh* mesh) { return mesh ? (mesh->n_elem + 127) / 128 : -1; }
+
+int nzb_gen_rate(const nzb_gen_mesh* mesh, const nzb_physics* phys, int unfolded, const double* U, double* out,
+                 double* wave, double* fw, double* smax, void* stream) {
+  if (check_gen(mesh, phys)) return -1;
+  if (!U || !out || !fw || !smax) return fail("gen_rate: null array");
+  if (unfolded ? (!mesh->grad_x || !mesh->grad_y) : (!mesh->grad_x_m || !mesh->grad_y_m || !mesh->face_basis_m))
+    return fail("gen_rate: the mesh lacks the operators of this mode");
+  return cuda_check(gen_rate_launch(*mesh, *phys, unfolded, U, out, wave, fw, smax, (cudaStream_t)stream),
+                    "generic rate launch");
+}
+
+int nzb_gen_limit(const nzb_gen_mesh* mesh, const nzb_physics* phys, double* U, unsigned long long* counters,
+                  void* stream) {
+  if (check_gen(mesh, phys)) return -1;
+  if (!U || !mesh->mean_weights) return fail("gen_limit: null array");
+  if (phys->limiter != 1) return 0;
+  return cuda_check(gen_limit_launch(*mesh, *phys, U, counters, (cudaStream_t)stream), "generic limiter launch");
+}
+
+int nzb_gen_update(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_update_args* args, void* stream) {
+  if (check_gen(mesh, phys)) return -1;
+  if (!args || !args->V || !args->F || !args->dt || !args->out || (args->a != 0.0 && !args->U0) ||
+      (args->stage == 1 && (!args->wave || !mesh->elem_area)))
+    return fail("gen_update: null array");
+  return cuda_check(gen_update_launch(*mesh, *phys, *args, (cudaStream_t)stream), "generic update launch");
+}
+
 int nzb_initial_state(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_initial_args* args, void* stream) {
   if (check_mesh(mesh)) return -1;
   if (!phys || !args || !args->verts || !args->wall || !args->q1d || !args->q1d_begin || !args->out)

@@ -25,6 +25,12 @@ NZB_INTERNAL cudaError_t observables_launch_quad(const nzb_mesh& m, const nzb_ph
                                                  cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_tri(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t geometry_launch_quad(const nzb_mesh& m, const nzb_geometry_args& a, cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_rate_launch(const nzb_gen_mesh& m, const nzb_physics& ph, int unfolded, const double* U,
+                                         double* out, double* wave, double* fw, double* smax, cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_limit_launch(const nzb_gen_mesh& m, const nzb_physics& ph, double* U,
+                                          unsigned long long* counters, cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_update_launch(const nzb_gen_mesh& m, const nzb_physics& ph, const nzb_gen_update_args& a,
+                                           cudaStream_t st);
 NZB_INTERNAL cudaError_t initial_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,
                                             cudaStream_t st);
 NZB_INTERNAL cudaError_t initial_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,

@@ -459,6 +459,68 @@ typedef struct {
 } nzb_initial_args;
 int nzb_initial_state(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_initial_args* args, void* stream);
 
+/* ---- any order, curved (Q = 2) elements: the reference's per-element operators
+ *
+ * The kernels above take straight-sided elements of order 0..3 with their
+ * tables in constant memory.  These entry points take what the reference's
+ * build_operators produces (src/spatial/operators.py:139-206), for any order
+ * and geometry order, in its layout: the state is (E, NP, 4), per element
+ * grad_x / grad_y (E, NP, NQV) (weak-form gradients w det (dphi/dx, dphi/dy)),
+ * grad_x_m / grad_y_m and face_basis_m (E, NF, NP, NQF) with the inverse mass
+ * folded in, per edge point the owner's normal (n_edge, NQF, 2) and
+ * |dX/dsigma| (n_edge, NQF).  Edges are numbered as the reference numbers
+ * them: interior first, then boundary (src/geometry/mesh.py:34-66).  All
+ * arrays device memory; NP up to 36 (triangles to p = 7, quadrilaterals to
+ * p = 5). */
+typedef struct {
+  int32_t np, nqv, nqf, nface;
+  int64_t n_elem, n_int, n_bnd;
+  const double* phi_vol;      /* (NP, NQV) */
+  const double* phi_face;     /* (2, NF, NP, NQF): side 0 owner's points, side 1 reversed */
+  const double* w_face;       /* (NQF) */
+  const double* grad_x;       /* (E, NP, NQV) */
+  const double* grad_y;
+  const double* grad_x_m;     /* (E, NP, NQV) */
+  const double* grad_y_m;
+  const double* face_basis_m; /* (E, NF, NP, NQF) */
+  const int32_t* face_edge;   /* (E, NF) global edge id */
+  const int32_t* face_side;   /* (E, NF) 0 owner, 1 neighbour */
+  const double* face_sign;    /* (E, NF) +1 owner, -1 neighbour */
+  const int32_t* edge_elem;   /* (n_edge, 2) owner, neighbour (boundary edges: owner, owner) */
+  const int32_t* edge_face;   /* (n_edge, 2) local faces */
+  const int32_t* edge_tag;    /* (n_bnd) boundary tag of each boundary edge */
+  const double* edge_normal;  /* (n_edge, NQF, 2) */
+  const double* edge_jac;     /* (n_edge, NQF) */
+  const double* edge_length;  /* (n_edge) */
+  const double* elem_area;    /* (E) */
+  const double* mean_weights; /* (E, NP) cell-average weights */
+} nzb_gen_mesh;
+/* unfolded = 1: out = the residual R (src/backends/_numba_kernels.py:667-759, apply_mass false);
+ * 0: out = the rate -M^-1 R (:586-664).  wave (E, nullable) the wave-speed sums; fw (n_edge, NQF, 4)
+ * and smax (n_edge) scratch of the edge pass. */
+int nzb_gen_rate(const nzb_gen_mesh* mesh, const nzb_physics* phys, int unfolded, const double* U, double* out,
+                 double* wave, double* fw, double* smax, void* stream);
+/* The positivity limiter in place (src/backends/_numba_kernels.py:927-1093); counters (device 2 x
+ * uint64, nullable) accumulate the scaled and repaired elements. */
+int nzb_gen_limit(const nzb_gen_mesh* mesh, const nzb_physics* phys, double* U, unsigned long long* counters,
+                  void* stream);
+/* One stage's update: stage 1 sets dt = dt_factor 2 A / max(wave, 1e-10) and the per-block partial
+ * sums of the weighted squares of F (partial: nzb_gen_blocks(mesh) doubles, nullable); then
+ * out = a U0 + b (V + dt F), or V + dt F when a = 0 (src/backends/_numba_kernels.py:789-850). */
+typedef struct {
+  int32_t stage, pad;
+  double dt_factor, a, b;
+  const double* V;
+  const double* U0;
+  const double* F;
+  const double* wave;
+  double* dt;
+  double* out;
+  double* partial;
+} nzb_gen_update_args;
+int nzb_gen_update(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_update_args* args, void* stream);
+int64_t nzb_gen_blocks(const nzb_gen_mesh* mesh);
+
 const char* nzb_last_error(void);
 int nzb_version(void);
 
