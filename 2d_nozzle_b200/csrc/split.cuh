@@ -547,6 +547,9 @@ __global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
   int inst = -1;
   if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
   const bool active = e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0);
+  // a block whose 32 elements are all retired (or past the end) has nothing to do: it leaves before
+  // its first barrier, together (the test is block-uniform)
+  if (!__syncthreads_or(active)) return;
   const double g = ph.gamma;
   double* const col = smem + L::U + lane;  // this lane's state column, stride 32
   double* const s_pfe = smem + L::PFE;

