@@ -35,7 +35,7 @@ from . import capi
 from . import nozzle as nz
 from .backend import B200Backend
 from .config import SolverOptions, step_coefficient
-from .autotune import choose_variant, set_struct_variant, tail_elements
+from .autotune import choose_variant, context_for, set_struct_variant, tail_elements
 from .layout import DeviceMesh, face_tangent_table, physics_struct
 from .march import solve as march_solve
 from .mesh import INFLOW, OUTFLOW
@@ -59,12 +59,12 @@ def from_soa(a, E, NP):
 class AdjointModel:
     """One mesh on the device, with what the transposed products need."""
 
-    def __init__(self, ops, flow, opts, device=None, variants: str = "single"):
+    def __init__(self, ops, flow, opts, device=None, variants: str = "auto"):
         self.ops, self.flow, self.opts = ops, flow, opts
         self.lib = capi.load()
-        self.variants = variants
         self.mesh = DeviceMesh(ops, device)
-        choose_variant(self.mesh, variants)
+        self.variants = context_for(self.mesh.E, variants)
+        choose_variant(self.mesh, self.variants)
         self.device = self.mesh.device
         self.E, self.NP, self.NV = self.mesh.E, self.mesh.np_, self.mesh.nf
         self.phys = physics_struct(flow, opts, ops.ref)

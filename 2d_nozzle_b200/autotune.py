@@ -148,6 +148,17 @@ def tail_elements() -> int:
     return int(os.environ.get("NZB_TAIL_ELEMENTS", "32768"))
 
 
+def context_for(n_elem: int, variants: str = "auto") -> str:
+    """The variant context of one solve on a mesh of ``n_elem`` elements: ``auto`` takes the single-solve
+    (latency) choice for a mesh too small to fill the GPU and the batch (throughput) choice for a larger
+    one, with the same threshold as a batch's tail switch; ``single`` or ``batch`` forces one."""
+    if variants == "auto":
+        return "batch" if tail_elements() and n_elem > tail_elements() else "single"
+    if variants not in CONTEXTS:
+        raise ValueError(f"variants {variants!r}: use 'auto' or one of {CONTEXTS}")
+    return variants
+
+
 def choose_variant(mesh, context: str = "single") -> str:
     """Set ``mesh.split`` / ``mesh.edge_pass`` / ``mesh.vjp_split`` for its element type in a context
     (``single`` or ``batch``); returns the forward variant's name."""

@@ -30,7 +30,7 @@ import numpy as np
 
 from . import capi
 from .config import FLOOR, SCHEMES, recommended_scheme, step_coefficient
-from .autotune import choose_variant
+from .autotune import choose_variant, context_for
 from .layout import DeviceMesh, physics_struct
 
 
@@ -47,7 +47,7 @@ class B200Backend:
         return super().__new__(cls)
 
     def __init__(self, ops, flow, opts, *, device=None, force_general: bool = False, device_metrics: bool = False,
-                 variants: str = "single"):
+                 variants: str = "auto"):
         import torch
 
         self.torch = torch
@@ -80,7 +80,8 @@ class B200Backend:
         self._solvers: dict[str, int] = {}
         self._obs = None
         # fused or edge-pass face fluxes, fixed per element type
-        choose_variant(self.mesh, variants)
+        # launch variants: the latency choice for a mesh that cannot fill the GPU, else the throughput one
+        choose_variant(self.mesh, context_for(self.mesh.E, variants))
 
     def __del__(self):
         lib = getattr(self, "lib", None)

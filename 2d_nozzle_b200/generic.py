@@ -37,7 +37,7 @@ def needs_generic(ops) -> bool:
 class GenericB200Backend(B200Backend):
     name = "b200"
 
-    def __init__(self, ops, flow, opts, *, device=None, variants: str = "single", **_):
+    def __init__(self, ops, flow, opts, *, device=None, variants: str = "auto", **_):
         import torch
 
         self.torch = torch
