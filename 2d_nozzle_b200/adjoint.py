@@ -591,10 +591,13 @@ class BatchGradient:
     """
 
     def __init__(self, case: DifferentiableCase, members, objective="thrust", names=None, device=None,
-                 variants: str = "batch"):
+                 variants: str = "batch", compact: bool = True):
+        """``compact``: late in the marches, launch only the blocks that hold elements of members still
+        marching (the same kernels on the same elements: the same bits)."""
         from .batch import Instance
 
         self.variants = variants
+        self.compact = bool(compact)
 
         self.case = case
         self.members = [dict(m) for m in members]
@@ -638,7 +641,7 @@ class BatchGradient:
         marching), at a point that depends on the whole batch, so the two
         orders agree to round-off.
         """
-        from .batch import BatchSolver
+        from .batch import BatchSolver, blocks_of
 
         import time
 
@@ -652,7 +655,7 @@ class BatchGradient:
             clock.append(time.perf_counter())
             self.timings[name] = self.timings.get(name, 0.0) + clock[-1] - clock[-2]
 
-        fwd = BatchSolver(self.instances, device=dev, variants=self.variants)
+        fwd = BatchSolver(self.instances, device=dev, variants=self.variants, compact=self.compact)
         if len(fwd.meshes) != 1:
             raise NotImplementedError("the members of one batch share the element kind and order")
         dm = fwd.meshes[0]
@@ -694,24 +697,45 @@ class BatchGradient:
         am.tolerance = float(adjoint_tolerance)
         am.max_iterations = int(max_iterations)
         offs = np.zeros(1, np.int64)
-        h = capi.P()
-        capi.check(lib.nzb_adjoint_create(1, C.byref(mesh), C.byref(ph), C.byref(bf), offs.ctypes.data, C.byref(am),
-                                          C.byref(h)), "nzb_adjoint_create")
-        # the adjoint's tail: a second march object over the same buffers with the single-solve variant,
-        # taken once the members still marching (and those that may yet start) hold few elements
-        cur = [h.value]
-        h_tail = None
-        tail_at = tail_elements() if self.variants == "batch" else 0
-        mesh_t = capi.Mesh()
-        C.memmove(C.byref(mesh_t), C.byref(mesh), C.sizeof(capi.Mesh))
-        set_struct_variant(mesh_t, dm.kind, dm.order, "single")
-        if tail_at and mesh_t.vjp_split != mesh.vjp_split:
-            ht = capi.P()
-            capi.check(lib.nzb_adjoint_create(1, C.byref(mesh_t), C.byref(ph), C.byref(bf), offs.ctypes.data,
-                                              C.byref(am), C.byref(ht)), "nzb_adjoint_create (tail)")
-            h_tail = ht.value
         elem_count = np.asarray([hi - lo for lo, hi in spans], np.int64)
+        handles = {}  # adjoint march object -> its block list (kept alive with it)
+
+        def variant_mesh(context):
+            mc = capi.Mesh()
+            C.memmove(C.byref(mc), C.byref(mesh), C.sizeof(capi.Mesh))
+            if context is not None:
+                set_struct_variant(mc, dm.kind, dm.order, context)
+            return mc
+
+        def blocks_for(context, mask):
+            W = int(lib.nzb_block_width(C.byref(variant_mesh(context)), 1))
+            return blocks_of([spans[i] for i in range(n) if mask[i]] if mask is not None else [(0, E)], W)
+
+        def adjoint_handle(context, mask):
+            """An adjoint march object over the shared buffers: the bucket's batch variant, or that of
+            ``context``; with ``mask``, launching only the blocks that hold those members' elements.
+            Returns the object and the blocks one launch spans."""
+            mc = variant_mesh(context)
+            blocks = blocks_for(context, mask)
+            keep = None
+            if mask is not None:
+                keep = torch.as_tensor(blocks if blocks.size else np.zeros(1, np.int32), device=dev)
+                mc.vjp_blocks, mc.n_vjp_blocks = keep.data_ptr(), int(blocks.size)
+            hh = capi.P()
+            capi.check(lib.nzb_adjoint_create(1, C.byref(mc), C.byref(ph), C.byref(bf), offs.ctypes.data,
+                                              C.byref(am), C.byref(hh)), "nzb_adjoint_create")
+            handles[hh.value] = keep
+            return hh.value, int(blocks.size)
+
+        # Late in the march (few members left, or few blocks holding them) the adjoint switches to the
+        # single-solve variant and to a march object that lists only the blocks of members still
+        # marching or yet to start, as the forward batch does (BatchSolver._retarget).
+        first_h, launched = adjoint_handle(None, None)
+        cur = [first_h]
+        tail_at = tail_elements() if self.variants == "batch" else 0
+        in_tail = False
         self.tail_switched = {"forward": None, "adjoint": None}
+        self.compactions = {"forward": 0, "adjoint": 0}
         coef = step_coefficient(self.cases[0].operators.ref.order, self.case.options.cfl, "ssprk3")
         started = np.zeros(n, bool)
         elem_inst = dm.elem_inst_t
@@ -795,26 +819,36 @@ class BatchGradient:
                     break
                 if fwd_running:
                     fwd_running = fwd.n_running() if fwd.done < fwd.opts.max_iterations else 0
-                    fwd._maybe_tail(fwd_running)
-                    if fwd.handle != fwd._main and self.tail_switched["forward"] is None:
-                        self.tail_switched["forward"] = fwd.done
+                    fwd._retarget(fwd_running)
+                    self.tail_switched["forward"] = fwd.tail_switched_at
+                    self.compactions["forward"] = fwd.compactions
                 if adj_running:
                     adj_running = int(t["n_running"].item())
-                    if h_tail is not None and cur[0] != h_tail and adj_running:
-                        ast_now = status.cpu().numpy()
-                        pending = fwd.t["status"].cpu().numpy() == 0
-                        if int(elem_count[(ast_now == 0) | pending].sum()) <= tail_at:
-                            cur[0] = h_tail
-                            self.tail_switched["adjoint"] = int(t["iterations"].max().item())
+                    if adj_running:
+                        # members marching, still in their forward solve, or converged and not started yet
+                        fst_now = fwd.t["status"].cpu().numpy()
+                        mask = (status.cpu().numpy() == 0) | (fst_now == 0) | ((fst_now == 1) & ~started)
+                        tail = in_tail or (tail_at > 0 and int(elem_count[mask].sum()) <= tail_at)
+                        need = int(blocks_for("single" if tail else None, mask).size)
+                        if tail != in_tail or (self.compact and 2 * need <= launched):
+                            old_h = cur[0]
+                            cur[0], launched = adjoint_handle("single" if tail else None,
+                                                              mask if self.compact else None)
+                            lib.nzb_adjoint_destroy(old_h)
+                            del handles[old_h]
+                            self.compactions["adjoint"] += 1
+                            if tail and not in_tail:
+                                in_tail = True
+                                self.tail_switched["adjoint"] = int(t["iterations"].max().item())
                     if nf:
                         t_f = ev[0].elapsed_time(ev[1]) / nf
                         t_a = ev[2].elapsed_time(ev[3])
                         per_round = max(1, min(64, int(round(t_a / max(t_f, 1e-3)))))
             lap("adjoint" if not overlap else "forward+adjoint")
         finally:
-            lib.nzb_adjoint_destroy(h.value)
-            if h_tail is not None:
-                lib.nzb_adjoint_destroy(h_tail)
+            for hh in list(handles):
+                lib.nzb_adjoint_destroy(hh)
+            handles.clear()
         fres = fwd.results(with_state=False)
         ast = status.cpu().numpy()
         its = t["iterations"].cpu().numpy()

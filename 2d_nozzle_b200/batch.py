@@ -54,11 +54,21 @@ class InstanceResult:
     U: np.ndarray | None
 
 
+def blocks_of(ranges, width: int) -> np.ndarray:
+    """The sorted block indices (``width`` elements per block) that hold an element of any of the
+    half-open element ranges."""
+    idx = [np.arange(lo // width, (hi - 1) // width + 1) for lo, hi in ranges if hi > lo]
+    if not idx:
+        return np.zeros(0, np.int32)
+    return np.unique(np.concatenate(idx)).astype(np.int32)
+
+
 class BatchSolver:
-    def __init__(self, instances: list[Instance], device=None, variants: str = "batch"):
+    def __init__(self, instances: list[Instance], device=None, variants: str = "batch", compact: bool = True):
         """``variants``: the launch variants' context in the variant table -- ``batch`` (measured on
         buckets marching side by side) or ``single`` (the one-solve choice, so a batch gives a plain
-        solve's bits)."""
+        solve's bits).  ``compact``: late in the march, launch only the blocks that hold elements of
+        running instances (the same kernels on the same elements: the same bits)."""
         import torch
 
         if not instances:
@@ -224,46 +234,84 @@ class BatchSolver:
         bm.max_iterations = int(opts0.max_iterations)
         self.bm = bm
         nb = len(self.meshes)
-        meshes = (capi.Mesh * nb)(*[dm.c for dm in self.meshes])
-        physs = (capi.Physics * nb)(*self.phys)
-        bufs = (capi.Buffers * nb)(*[b for b, _ in self.buffers])
-        offs = np.asarray(self.offsets, np.int64)
-        facs = np.asarray(self.factors, float)
-        h = capi.P()
-        capi.check(self.lib.nzb_batch_create(nb, meshes, physs, bufs, offs.ctypes.data, facs.ctypes.data, C.byref(bm),
-                                             C.byref(h)), "nzb_batch_create")
-        self.handle = h.value
-        self._main = self.handle
-        # the tail: once the instances still marching hold few elements, the batch's throughput variants
-        # leave the GPU idle and an element's latency decides -- a second march object over the same
-        # buffers runs the single-solve variants from then on (no object when they are the same)
-        self.variants = variants
-        self._tail = None
-        self._tail_at = tail_elements() if variants == "batch" else 0
+        self._physs = (capi.Physics * nb)(*self.phys)
+        self._bufs = (capi.Buffers * nb)(*[b for b, _ in self.buffers])
+        self._offs = np.asarray(self.offsets, np.int64)
+        self._facs = np.asarray(self.factors, float)
         self._elem_count = np.asarray(end - begin, np.int64)
-        tail_meshes = []
-        for dm in self.meshes:
-            mc = capi.Mesh()
-            C.memmove(C.byref(mc), C.byref(dm.c), C.sizeof(capi.Mesh))
-            set_struct_variant(mc, dm.kind, dm.order, "single")
-            tail_meshes.append(mc)
-        if self._tail_at and any((a.split, a.edge_pass, a.vjp_split) != (dm.c.split, dm.c.edge_pass, dm.c.vjp_split)
-                                 for a, dm in zip(tail_meshes, self.meshes)):
-            ht = capi.P()
-            capi.check(self.lib.nzb_batch_create(nb, (capi.Mesh * nb)(*tail_meshes), physs, bufs, offs.ctypes.data,
-                                                 facs.ctypes.data, C.byref(bm), C.byref(ht)), "nzb_batch_create (tail)")
-            self._tail = ht.value
+        self._handles = {}  # march object -> the block lists it launches (kept alive with it)
+        self._main = self._create(None, None)
+        self.handle = self._main
+        # Late in a march most instances have retired.  Two things follow, both taken between chunks when
+        # the set of running instances has changed: (1) once the instances still marching hold few
+        # elements, the batch's throughput variants leave the GPU idle and an element's latency decides,
+        # so the march switches to the single-solve variants (the tail); (2) once the blocks holding
+        # running elements are at most half of those a launch spans, a march object whose launches list
+        # only those blocks replaces the current one, so a launch no longer walks every retired block.
+        self.variants = variants
+        self._tail_at = tail_elements() if variants == "batch" else 0
+        self.compact = bool(compact)
+        self._in_tail = False
+        self._launched = self._blocks_launched(None, None)
         self.tail_switched_at = None  # iteration of the switch, if any
+        self.compactions = 0
         self._last_running = n
         self.done = 0
         self.chunks = 0
         self.launches = 0
         self._obs = None
 
+    def _meshes_for(self, context, running):
+        """Mesh descriptors for a march object -- the buckets' own variants, or those of ``context`` --
+        and, with ``running`` (a per-instance mask), each bucket's list of the blocks that hold elements
+        of running instances (None without)."""
+        meshes, lists = [], []
+        for dm, mem in zip(self.meshes, self.members):
+            mc = capi.Mesh()
+            C.memmove(C.byref(mc), C.byref(dm.c), C.sizeof(capi.Mesh))
+            if context is not None:
+                set_struct_variant(mc, dm.kind, dm.order, context)
+            blocks = None
+            if running is not None:
+                W = int(self.lib.nzb_block_width(C.byref(mc), 0))
+                blocks = blocks_of([(int(self.local[i]), int(self.local[i] + self._elem_count[i])) for i in mem
+                                    if running[i]], W)
+            meshes.append(mc)
+            lists.append(blocks)
+        return meshes, lists
+
+    def _blocks_launched(self, context, running) -> int:
+        meshes, lists = self._meshes_for(context, running)
+        return sum(int(self.lib.nzb_element_blocks(C.byref(m))) if b is None else int(b.size)
+                   for m, b in zip(meshes, lists))
+
+    def _create(self, context, running) -> int:
+        meshes, lists = self._meshes_for(context, running)
+        keep = []
+        for mc, blocks in zip(meshes, lists):
+            if blocks is not None:
+                t = self.torch.as_tensor(blocks if blocks.size else np.zeros(1, np.int32), device=self.device)
+                mc.fwd_blocks, mc.n_fwd_blocks = t.data_ptr(), int(blocks.size)
+                keep.append(t)
+        nb = len(meshes)
+        h = capi.P()
+        capi.check(self.lib.nzb_batch_create(nb, (capi.Mesh * nb)(*meshes), self._physs, self._bufs,
+                                             self._offs.ctypes.data, self._facs.ctypes.data, C.byref(self.bm),
+                                             C.byref(h)), "nzb_batch_create")
+        self._handles[h.value] = keep
+        # buckets with nothing to launch (every block of theirs retired) make no launches
+        self._bucket_live = [b is None or b.size > 0 for b in lists]
+        return h.value
+
+    def _drop(self, h) -> None:
+        if h and h in self._handles and h != getattr(self, "_main", None):
+            self.lib.nzb_batch_destroy(h)
+            del self._handles[h]
+
     def __del__(self):
-        for h in (getattr(self, "_main", None), getattr(self, "_tail", None)):
-            if h:
-                self.lib.nzb_batch_destroy(h)
+        for h in list(getattr(self, "_handles", {})):
+            self.lib.nzb_batch_destroy(h)
+        self._handles = {}
 
     @property
     def _stream(self):
@@ -272,7 +320,8 @@ class BatchSolver:
     def launches_per_chunk(self, n: int) -> int:
         """Kernel launches of one n-step chunk: 3 stages (SSP-RK3) or a stage and a copy (Euler) per
         bucket and step, plus the check."""
-        return sum((3 if dm.order > 0 else 2) * n for dm in self.meshes) + 1
+        live = getattr(self, "_bucket_live", [True] * len(self.meshes))
+        return sum((3 if dm.order > 0 else 2) * n for dm, on in zip(self.meshes, live) if on) + 1
 
     def launch_chunk(self, n: int, first: bool) -> None:
         """Queue one n-step chunk (and its retirement check) on the current stream; no synchronisation."""
@@ -290,24 +339,44 @@ class BatchSolver:
         st = self.t["status"].cpu().numpy()
         return int(self._elem_count[st == 0].sum())
 
-    def _maybe_tail(self, running: int) -> None:
-        if self._tail is None or self.handle == self._tail or running == self._last_running:
+    def _retarget(self, running: int) -> None:
+        """Between chunks (nothing queued): the tail switch and the block-list compaction."""
+        if running == self._last_running or not running:
             return
         self._last_running = running
-        if running and self.active_elements() <= self._tail_at:
-            self.handle = self._tail
-            self.tail_switched_at = self.done
+        mask = self.t["status"].cpu().numpy() == 0
+        tail = self._in_tail or (self._tail_at > 0 and int(self._elem_count[mask].sum()) <= self._tail_at)
+        context = "single" if tail else None
+        if not self.compact:
+            mask = None
+        need = self._blocks_launched(context, mask)
+        if tail != self._in_tail or (mask is not None and 2 * need <= self._launched):
+            old = self.handle
+            self.handle = self._create(context, mask)
+            self._drop(old)
+            self._launched = need
+            self.compactions += 1
+            if tail and not self._in_tail:
+                self._in_tail = True
+                self.tail_switched_at = self.done
+
+    _maybe_tail = _retarget
 
     def step_chunk(self, n: int, first: bool) -> int:
         self.launch_chunk(n, first)
         running = self.n_running()
-        self._maybe_tail(running)
+        self._retarget(running)
         return running
 
     def reset(self) -> None:
         """Put every instance back at its initial state with a fresh march record."""
+        self._drop(self.handle)
         self.handle = self._main
+        self._bucket_live = [True] * len(self.meshes)
+        self._in_tail = False
+        self._launched = self._blocks_launched(None, None)
         self.tail_switched_at = None
+        self.compactions = 0
         self._last_running = len(self.instances)
         for (bf, S), U0 in zip(self.buffers, self.U0_soa):
             S[0].copy_(U0)

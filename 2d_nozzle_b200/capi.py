@@ -48,6 +48,10 @@ class Mesh(C.Structure):
         ("n_inst", I32),
         ("vjp_split", I32),
         ("reserved", I32),
+        ("fwd_blocks", P),
+        ("n_fwd_blocks", I64),
+        ("vjp_blocks", P),
+        ("n_vjp_blocks", I64),
     ]
 
 
@@ -262,6 +266,7 @@ SIGNATURES = [
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),
     ("nzb_element_blocks", I64, [C.POINTER(Mesh)]),
+    ("nzb_block_width", I64, [C.POINTER(Mesh), I32]),
     ("nzb_norm_finalize", C.c_int, [P, I64, C.c_double, P, P]),
     ("nzb_norm", C.c_int, [P, I64, C.c_int, P, P, P, P]),
     ("nzb_norm_noalloc", C.c_int, [P, I64, C.c_int, P, P, P]),

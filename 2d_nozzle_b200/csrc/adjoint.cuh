@@ -121,7 +121,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, VjpBounds<K, P>::MINB)
   __shared__ double vacc[NP * 4 * BT];  // vacc[(i * 4 + s) * BT + t]
   const int t = threadIdx.x;
   const int64_t E = m.n_elem;
-  const int64_t e = (int64_t)blockIdx.x * BT + t;
+  const int64_t blk = listed_block(m.vjp_blocks, E, BT);
+  const int64_t e = blk * BT + t;
   int inst = -1;
   if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
   const bool active = e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0);
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, VjpBounds<K, P>::MINB)
       }
     }
   }
-  if (w.mode == ADJ_DEFECT && w.norm_partial) block_sum_store<BT / 32>(dsq, w.norm_partial + blockIdx.x);
+  if (w.mode == ADJ_DEFECT && w.norm_partial) block_sum_store<BT / 32>(dsq, w.norm_partial + blk);
 }
 
 template <int K, int P>

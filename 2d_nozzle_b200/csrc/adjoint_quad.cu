@@ -8,13 +8,13 @@ template <int K, int P, bool AFF>
 cudaError_t launch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
   if constexpr (P > 0) {
     if (m.vjp_split == SPLIT_T) {
-      const unsigned nb = (unsigned)((m.n_elem + SPLIT_EB - 1) / SPLIT_EB);
-      k_vjp_split<K, P, AFF><<<nb, SPLIT_T * 32, VjpSplitSmem<K, P>::BYTES, st>>>(m, ph, w);
+      const unsigned nb = (unsigned)(m.vjp_blocks ? m.n_vjp_blocks : (m.n_elem + SPLIT_EB - 1) / SPLIT_EB);
+      if (nb) k_vjp_split<K, P, AFF><<<nb, SPLIT_T * 32, VjpSplitSmem<K, P>::BYTES, st>>>(m, ph, w);
       return cudaGetLastError();
     }
   }
-  const int64_t nb = (m.n_elem + Launch<K, P>::NT - 1) / Launch<K, P>::NT;
-  k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
+  const int64_t nb = m.vjp_blocks ? m.n_vjp_blocks : (m.n_elem + Launch<K, P>::NT - 1) / Launch<K, P>::NT;
+  if (nb) k_vjp<K, P, AFF><<<(unsigned)nb, Launch<K, P>::NT, 0, st>>>(m, ph, w);
   return cudaGetLastError();
 }
 

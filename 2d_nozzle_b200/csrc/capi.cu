@@ -77,17 +77,28 @@ static int block_threads(int kind, int order) {
   }
   return 128;
 }
-// Blocks of the forward element kernel (= norm partial slots of stage 1):
-// 32 elements per block with four threads per element.
-static int64_t element_blocks(const nzb_mesh& m) {
-  const int bt = (m.split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
-  return (m.n_elem + bt - 1) / bt;
+// Elements per block of the forward element kernel: 32 with four threads per
+// element, else one per thread.
+static int element_width(const nzb_mesh& m) {
+  return (m.split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
 }
-// Blocks of the adjoint state kernel (= defect partial slots): one thread per
-// element, or 32 elements per block with four threads per element.
-static int64_t adjoint_blocks(const nzb_mesh& m) {
-  const int bt = (m.vjp_split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
-  return (m.n_elem + bt - 1) / bt;
+// ... and of the adjoint state kernel.
+static int adjoint_width(const nzb_mesh& m) {
+  return (m.vjp_split == SPLIT_T && m.order > 0) ? SPLIT_EB : block_threads(m.kind, m.order);
+}
+// Blocks of the forward element kernel (= norm partial slots of stage 1).
+static int64_t element_blocks(const nzb_mesh& m) { return (m.n_elem + element_width(m) - 1) / element_width(m); }
+// Blocks of the adjoint state kernel (= defect partial slots).
+static int64_t adjoint_blocks(const nzb_mesh& m) { return (m.n_elem + adjoint_width(m) - 1) / adjoint_width(m); }
+
+// A block list (fwd_blocks / vjp_blocks) may list each of the mesh's blocks
+// at most once, and leaves block-partial norms undefined.
+static int check_block_list(const int32_t* list, int64_t n, int64_t blocks, const double* norm_partial,
+                            const char* what) {
+  if (!list) return 0;
+  if (n < 0 || n > blocks) return fail(std::string(what) + ": the block count must lie in [0, blocks of the mesh]");
+  if (norm_partial) return fail(std::string(what) + ": block-partial norms need every block (no block list)");
+  return 0;
 }
 
 // The element kernels live in forward_tri.cu / forward_quad.cu.
@@ -98,6 +109,7 @@ static int dispatch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cud
     return fail("the edge pass needs edge_conn, edge_flux and edge_speed");
   if (m.edge_pass && (reinterpret_cast<uintptr_t>(m.edge_flux) & 15) != 0)
     return fail("edge_flux must be 16-byte aligned");
+  if (check_block_list(m.fwd_blocks, m.n_fwd_blocks, element_blocks(m), w.norm_partial, "fwd_blocks")) return -1;
   if (ph.limiter == 2 && m.order > 0 && (w.op == OP_STAGE || w.op == OP_LIMIT)) {
     if (m.elem_inst && (m.n_inst < 1 || !m.inst_status))
       return fail("the Superbee limiter in a batch needs n_inst (lim_scale holds 4 per instance) and inst_status");
@@ -361,6 +373,7 @@ struct Batch {
 static int enqueue_bucket_step(const Batch& B, size_t b, cudaStream_t st) {
   {
     const nzb_mesh& m = B.mesh[b];
+    if (m.fwd_blocks && m.n_fwd_blocks == 0) return 0;  // every instance of the bucket has retired
     const nzb_buffers& bf = B.buf[b];
     const bool ssp = m.order > 0;
     Work w{};
@@ -439,6 +452,7 @@ static int batch_graph(Batch& B, int n, int first, cudaGraphExec_t* out) {
 // The adjoint kernels live in adjoint_tri.cu / adjoint_quad.cu.
 static int dispatch_vjp(const nzb_mesh& m, const nzb_physics& ph, const AdjWork& w, cudaStream_t st) {
   if (adjoint_blocks(m) > 0x7fffffff) return fail("too many elements for one launch");
+  if (check_block_list(m.vjp_blocks, m.n_vjp_blocks, adjoint_blocks(m), w.norm_partial, "vjp_blocks")) return -1;
   const cudaError_t e = m.kind == NZB_TRI ? vjp_launch_tri(m, ph, w, st) : vjp_launch_quad(m, ph, w, st);
   return cuda_check(e, "vjp kernel launch");
 }
@@ -832,6 +846,11 @@ int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_arg
 int64_t nzb_norm_blocks(int64_t n_elem) { return n_elem <= 0 ? 0 : (n_elem + SPLIT_EB - 1) / SPLIT_EB; }
 
 int64_t nzb_element_blocks(const nzb_mesh* mesh) { return mesh ? element_blocks(*mesh) : -1; }
+
+int64_t nzb_block_width(const nzb_mesh* mesh, int which) {
+  if (!mesh || (which != 0 && which != 1)) return -1;
+  return which == 0 ? element_width(*mesh) : adjoint_width(*mesh);
+}
 
 int nzb_norm_finalize(const double* partial, int64_t n_partial, double count, double* out, void* stream) {
   if (!partial || !out || n_partial <= 0 || !(count > 0)) return fail("norm_finalize: bad arguments");

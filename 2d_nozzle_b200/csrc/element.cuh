@@ -323,6 +323,17 @@ __device__ __forceinline__ void limit_element(const A& u, const nzb_mesh& m,
   scaled = 1;
 }
 
+// The block of the mesh this CTA runs: entry blockIdx.x of a block list (the
+// blocks of a batch that still hold marching elements), or blockIdx.x itself.
+// An entry outside [0, ceil(E / W)) maps to the first block past the end, whose
+// elements are all inactive.
+__device__ __forceinline__ int64_t listed_block(const int32_t* __restrict__ list, int64_t E, int W) {
+  if (!list) return blockIdx.x;
+  const int64_t end = (E + W - 1) / W;
+  const int64_t b = __ldg(list + blockIdx.x);
+  return (b < 0 || b > end) ? end : b;
+}
+
 template <int NW>
 __device__ __forceinline__ void block_sum_store(double v, double* dst) {
   __shared__ double red[NW];
@@ -464,7 +475,8 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
   __shared__ double facc[NP * 4 * BT];
   const int t = threadIdx.x;
   const int64_t E = m.n_elem;
-  const int64_t e = (int64_t)blockIdx.x * BT + t;
+  const int64_t blk = listed_block(m.fwd_blocks, E, BT);
+  const int64_t e = blk * BT + t;
   // a retired instance of a batch is left untouched
   int inst = -1;
   if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
@@ -769,7 +781,7 @@ __global__ void __launch_bounds__(Launch<K, P>::NT, LIM ? Launch<K, P>::MINB_STA
   }
   // block-level reductions (every thread of the block reaches these)
   if (LIM && w.op == OP_STAGE && w.norm_partial && w.stage == 1)
-    block_sum_store<BT / 32>(nrm, w.norm_partial + blockIdx.x);
+    block_sum_store<BT / 32>(nrm, w.norm_partial + blk);
   if (LIM && (w.op == OP_STAGE || w.op == OP_LIMIT) && w.counters) {
     const int ns = __syncthreads_count(scaled);
     const int nr = __syncthreads_count(repaired);

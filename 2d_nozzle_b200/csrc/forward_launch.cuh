@@ -41,9 +41,11 @@ cudaError_t launch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cuda
   bool done = false;
   if constexpr (P > 0) {
     if (m.split == SPLIT_T) {
-      const unsigned nb = (unsigned)((m.n_elem + SPLIT_EB - 1) / SPLIT_EB);
+      const unsigned nb = (unsigned)(m.fwd_blocks ? m.n_fwd_blocks : (m.n_elem + SPLIT_EB - 1) / SPLIT_EB);
       constexpr int SM = SplitSmem<K, P>::BYTES;
-      if (lim)
+      if (nb == 0)
+        ;  // an empty block list: nothing marches
+      else if (lim)
         k_split<K, P, AFF, true><<<nb, SPLIT_T * 32, SM, st>>>(m, ph, w);
       else
         k_split<K, P, AFF, false><<<nb, SPLIT_T * 32, SM, st>>>(m, ph, w);
@@ -52,14 +54,16 @@ cudaError_t launch(const nzb_mesh& m, const nzb_physics& ph, const Work& w, cuda
   }
   if (!done) {
     constexpr int NT = Launch<K, P>::NT;
-    const unsigned nb = (unsigned)((m.n_elem + NT - 1) / NT);
+    const unsigned nb = (unsigned)(m.fwd_blocks ? m.n_fwd_blocks : (m.n_elem + NT - 1) / NT);
     const bool ep = m.edge_pass && w.op != OP_LIMIT;
     if (ep) {
       k_edge<K, P><<<(unsigned)((m.n_edge + 127) / 128), 128, 0, st>>>(m, ph, w.V);
       const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
-    if (lim && ep)
+    if (nb == 0)
+      ;  // an empty block list: nothing marches
+    else if (lim && ep)
       k_element<K, P, AFF, true, true><<<nb, NT, 0, st>>>(m, ph, w);
     else if (lim)
       k_element<K, P, AFF, true, false><<<nb, NT, 0, st>>>(m, ph, w);

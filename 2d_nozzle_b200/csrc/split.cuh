@@ -543,7 +543,8 @@ __global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
   extern __shared__ double smem[];
   const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
   const int64_t E = m.n_elem;
-  const int64_t e = (int64_t)blockIdx.x * EB + lane;
+  const int64_t blk = listed_block(m.fwd_blocks, E, EB);
+  const int64_t e = blk * EB + lane;
   int inst = -1;
   if (e < E && m.elem_inst) inst = __ldg(m.elem_inst + e);
   const bool active = e < E && (inst < 0 || __ldg(m.inst_status + inst) == 0);
@@ -824,7 +825,7 @@ __global__ void __launch_bounds__(SPLIT_T * 32, SplitSmem<K, P>::MINB)
       for (int k = 0; k < SPLIT_T; ++k) tot += smem[L::NRM + k * EB + lane];
       if (w.elem_norm && active) w.elem_norm[e] = tot;
     }
-    if (w.norm_partial) block_sum_store<SPLIT_T>(tot, w.norm_partial + blockIdx.x);
+    if (w.norm_partial) block_sum_store<SPLIT_T>(tot, w.norm_partial + blk);
   }
 
   // ---- phase C: the positivity limiter (limiter 1), every warp for its lane's element

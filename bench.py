@@ -410,35 +410,43 @@ def adjoint_section(args, torch):
     batch = pkg("batch")
     cs0 = dc.case_at(members[0])
     inst0 = batch.Instance(cs0.operators, cs0.flow, dc.options, cs0.initial_state(), float(cs0.geometry.length))
-    bk, U0, _ = plain_solve(inst0, torch)
     ci = dc.options.check_interval
-    bk._S[0].copy_(U0)
-    bk.run_device(1)
-    bk.run_device(ci)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(10):
+
+    def per_iteration(variants):
+        """Seconds per plain forward iteration and per plain adjoint RK4 step of member 0."""
+        bk, U0, _ = plain_solve(inst0, torch, variants=variants)
+        bk._S[0].copy_(U0)
+        bk.run_device(1)
         bk.run_device(ci)
-        float(bk._res.item())
-    t_fwd = (time.perf_counter() - t0) / (10 * ci)
-    model = ad.AdjointModel(cs0.operators, cs0.flow, dc.options)
-    U_soa = ad.to_soa(torch.as_tensor(np.asarray(cs0.initial_state()), device="cuda"))
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(0)
-    am = ad.AdjointMarch(model, U_soa, torch.randn(U_soa.shape, generator=gen, dtype=torch.float64, device="cuda"),
-                         dc.options.cfl)
-    am._create(1e-300, 10**9)
-    am.run(0)
-    am.run(100)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            bk.run_device(ci)
+            float(bk._res.item())
+        t_f = (time.perf_counter() - t0) / (10 * ci)
+        model = ad.AdjointModel(cs0.operators, cs0.flow, dc.options, variants=variants)
+        U_soa = ad.to_soa(torch.as_tensor(np.asarray(cs0.initial_state()), device="cuda"))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(0)
+        am = ad.AdjointMarch(model, U_soa, torch.randn(U_soa.shape, generator=gen, dtype=torch.float64,
+                                                       device="cuda"), dc.options.cfl)
+        am._create(1e-300, 10**9)
+        am.run(0)
         am.run(100)
-    t_adj = (time.perf_counter() - t0) / 500
-    del am, bk
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            am.run(100)
+        t_a = (time.perf_counter() - t0) / 500
+        del am, bk
+        return t_f, t_a
+
+    t_fwd, t_adj = per_iteration("single")
+    t_fwd_b, t_adj_b = per_iteration("batch")
     cost = lambda r: r.forward_iterations * t_fwd + r.adjoint_iterations * t_adj  # noqa: E731
     fixed = max(0.0, (t_plain - sum(cost(out[i]) for i in sub)) / len(sub))
     est_all = sum(cost(r) for r in out) + fixed * len(out)
+    est_same = sum(r.forward_iterations * t_fwd_b + r.adjoint_iterations * t_adj_b for r in out) + fixed * len(out)
     return {"workload": f"{len(members)} bezier8 members (8 offsets, sigma 2% of the throat half-height, seed 0) "
                         f"around AR 2.5, tri p=2 refine 2 (2240 elements), AUSM+-up, forward and adjoint to 1e-10",
             "metric": "thrust gradients/s (8 design variables each)", "batched_gradients": len(ok),
@@ -450,12 +458,18 @@ def adjoint_section(args, torch):
             "max_rel_diff_batched_vs_plain": diff, "batched_phases_s": bg.timings,
             "phased_seconds": t_phased, "phased_phases_s": bg_p.timings, "max_rel_diff_overlapped_vs_phased": same,
             "tail_switch": {"overlapped": bg.tail_switched, "phased": bg_p.tail_switched},
+            "compactions": {"overlapped": bg.compactions, "phased": bg_p.compactions},
             "forward_status": {st: sum(r.forward_status == st for r in out) for st in {r.forward_status for r in out}},
             "forward_iteration_cap": args.adjoint_cap,
             "all_members_estimated_plain_seconds": est_all,
             "speedup_all_members": (len(ok) / t_batch) / max(len(ok) / est_all, 1e-300),
             "plain_cost_model": {"forward_s_per_iteration": t_fwd, "adjoint_s_per_iteration": t_adj,
-                                 "fixed_s_per_member": fixed}}
+                                 "fixed_s_per_member": fixed},
+            "same_kernels": {"note": "every member one at a time with the batch's kernel variants instead of the "
+                                     "single-solve (latency) ones, estimated the same way",
+                             "forward_s_per_iteration": t_fwd_b, "adjoint_s_per_iteration": t_adj_b,
+                             "all_members_estimated_plain_seconds": est_same,
+                             "speedup_all_members": (len(ok) / t_batch) / max(len(ok) / est_same, 1e-300)}}
 
 
 def vjp_micro(torch, n_members=64):
@@ -679,6 +693,7 @@ def run_ours(args, rank, world, torch, dist):
                    "elements": n_elem_all, "buckets_rank0": len(solver.meshes), "outcomes": outcomes,
                    "converged_per_step": n_conv_all, "l2": "flushed (256 MB write) before each sweep",
                    "tail_switch_iteration_rank0": solver.tail_switched_at,
+                   "block_list_compactions_rank0": solver.compactions,
                    "parallelism": (f"sweep of {args.points * world} points partitioned over {world} GPUs "
                                    f"({args.points} each, points r::{world})" if world > 1 else "1 GPU")},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

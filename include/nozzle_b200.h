@@ -123,6 +123,21 @@ typedef struct {
   int32_t n_inst;           /* instances of a batch (elem_inst values lie in [0, n_inst)); 0 or 1: one */
   int32_t vjp_split;        /* threads per element of the adjoint state kernel (nzb_vjp, nzb_adjoint_*): 0 or 1, or 4 */
   int32_t reserved;
+  /* Optional block lists (null: every block).  The forward element kernel
+   * (residuals, rates, stages, nzb_limit's positivity pass) and the adjoint
+   * state kernel (nzb_vjp, nzb_adjoint_*) then run only the listed blocks:
+   * block b holds elements [b W, (b + 1) W), W = nzb_block_width(mesh, 0) for
+   * the forward kernel and nzb_block_width(mesh, 1) for the adjoint one.  An
+   * element of an unlisted block is left as an element of a retired instance
+   * is: a batch lists the blocks that hold elements of instances still
+   * marching, so a launch late in a march no longer spans every retired block.
+   * Entries outside [0, ceil(n_elem / W)) are skipped; the edge pass, the
+   * Superbee passes and every other kernel ignore the lists; block-partial norms (norm_partial) are
+   * refused with a list, since unlisted blocks would leave stale partials. */
+  const int32_t* fwd_blocks;
+  int64_t n_fwd_blocks;
+  const int32_t* vjp_blocks;
+  int64_t n_vjp_blocks;
 } nzb_mesh;
 
 /* Gas, operating point and limiter constants, evaluated on the host exactly
@@ -203,6 +218,10 @@ int nzb_stage(const nzb_mesh* mesh, const nzb_physics* phys, const nzb_stage_arg
 int64_t nzb_norm_blocks(int64_t n_elem);
 /* Blocks (= partial-sum slots written by stage 1) of the element kernel. */
 int64_t nzb_element_blocks(const nzb_mesh* mesh);
+/* Elements per block W of the forward element kernel (which = 0) or of the
+ * adjoint state kernel (which = 1) for the mesh's variant (split, vjp_split):
+ * the unit of the fwd_blocks / vjp_blocks lists.  -1 for a bad argument. */
+int64_t nzb_block_width(const nzb_mesh* mesh, int which);
 /* out[0] = sqrt(sum partial[0..n_partial) / count) -- fixed summation order. */
 int nzb_norm_finalize(const double* partial, int64_t n_partial, double count, double* out, void* stream);
 /* Weighted RMS of a (4, NP, E) array: out[0] = sqrt(mean((w_s A)^2)).
