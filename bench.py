@@ -235,6 +235,19 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500, ki
     for name, t in results.items():
         b = alg["residual"] if name.startswith("residual") else (alg["stage1"] if name.startswith("stage1") else alg["stage23"])
         out["kernels"][name] = {"ms": t * 1e3, "alg_bytes_per_elem": b, "gbs": b * E / t / 1e9}
+    # FP64 operations per element (2 per DFMA, 1 per DADD or DMUL thread instruction; divisions and square
+    # roots count as the instructions they compile to), counted by ncu on 490,000 cubic triangles and 245,000
+    # cubic quadrilaterals of the same state distribution with the one-thread kernels (the stages' counts
+    # depend on how many elements the limiter works on, 53 % / 66 % here)
+    fp64 = {("tri", 3): {"residual_roe": 9067.1, "residual_hllc": 9323.5, "residual_ausmup": 8753.7,
+                         "stage1_hllc": 12996.2, "stage2_hllc": 12945.0, "stage3_hllc": 12938.8},
+            ("quad", 3): {"residual_roe": 13154.5, "residual_hllc": 13496.5, "residual_ausmup": 12721.2,
+                          "stage1_hllc": 21072.5, "stage2_hllc": 20930.6, "stage3_hllc": 20979.5}}.get((kind, order), {})
+    # nominal FP64 peak: 148 SMs x 64 FP64 lanes x 2 flops per FMA at 1965 MHz
+    peak_fp64 = 148 * 64 * 2 * 1.965e9 / 1e12
+    for name, t in results.items():
+        if name in fp64:
+            out["kernels"][name]["fp64_tflops"] = fp64[name] * E / t / 1e12
     dom = max(results, key=results.get)
     k = out["kernels"][dom]
     # DRAM bytes per element of each kernel from an ncu capture of 490,000 cubic triangles
@@ -246,6 +259,16 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500, ki
                        "traffic": traffic[dom] * E if dom in traffic else None,
                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on 490,000 elements, "
                                          "scaled by element count", "workload": out["workload"]}
+    if dom in fp64:
+        f = fp64[dom]
+        ach = f * E / results[dom] / 1e12
+        # arithmetic intensity above the FP64 ridge caps the attainable HBM fraction below 1
+        out["roofline"]["fp64"] = {
+            "flops_per_elem": f, "achieved_tflops": ach, "peak_tflops": peak_fp64, "frac": ach / peak_fp64,
+            "peak_source": "nominal (148 SMs x 64 FP64 lanes x 2 flops x 1965 MHz)",
+            "intensity_flop_per_byte": f / k["alg_bytes_per_elem"],
+            "ridge_flop_per_byte": peak_fp64 * 1e3 / peak_gbs,
+            "hbm_frac_at_fp64_peak": min(1.0, peak_fp64 * 1e12 / f * k["alg_bytes_per_elem"] / (peak_gbs * 1e9))}
     return out
 
 

@@ -71,3 +71,38 @@ def test_noalloc_norm_refuses_an_oversized_mesh(cuda):
     rc = lib.nzb_norm_noalloc(A.data_ptr(), 8_388_609, 1, w.ctypes.data, out.data_ptr(), ctypes.c_void_p(0))
     assert rc != 0
     assert b"exceeds its fixed scratch" in lib.nzb_last_error()
+
+
+def test_noalloc_norm_inside_a_captured_graph(cuda):
+    """After one call outside capture (which looks the fixed array's address up), the call can be
+    captured into a CUDA graph: each replay takes the norm of the array's contents at that time."""
+    torch = cuda
+    capi = pkg("capi")
+    lib = capi.load()
+    E, np_ = 50_000, 6
+    g = torch.Generator(device="cpu").manual_seed(5)
+    A = torch.randn(4 * np_ * E, generator=g, dtype=torch.float64).cuda()
+    w = np.array([1.0, 0.9, 0.9, 0.8])
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    capi.check(lib.nzb_norm_noalloc(A.data_ptr(), E, np_, w.ctypes.data, out.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream), "nzb_norm_noalloc (warm-up)")
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.graph(graph, stream=side):
+        capi.check(lib.nzb_norm_noalloc(A.data_ptr(), E, np_, w.ctypes.data, out.data_ptr(), side.cuda_stream),
+                   "nzb_norm_noalloc (captured)")
+    scratch = torch.zeros(int(lib.nzb_norm_blocks(E)) + 1, dtype=torch.float64, device="cuda")
+    ref = torch.zeros(1, dtype=torch.float64, device="cuda")
+    seen = set()
+    for k in range(3):
+        A.mul_(1.5)
+        graph.replay()
+        capi.check(lib.nzb_norm(A.data_ptr(), E, np_, w.ctypes.data, scratch.data_ptr(), ref.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream), "nzb_norm")
+        torch.cuda.synchronize()
+        assert float(out.item()) == float(ref.item()), k
+        seen.add(float(out.item()))
+    assert len(seen) == 3
+    del graph
