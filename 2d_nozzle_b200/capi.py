@@ -222,6 +222,13 @@ class GenMesh(C.Structure):
                     "edge_jac", "edge_length", "elem_area", "mean_weights")]
 
 
+class GenGeometryArgs(C.Structure):
+    _fields_ = [("ng", I32), ("reserved", I32)] + [
+        (n, P) for n in ("X", "elem_nodes", "w_vol", "dphi_dxi", "dphi_deta", "dgeom_dxi", "dgeom_deta", "dgeom_dsigma",
+                         "grad_x", "grad_y", "grad_x_m", "grad_y_m", "face_basis_m", "inv_mass", "elem_area",
+                         "mean_weights", "edge_normal", "edge_jac", "edge_length", "bad")]
+
+
 class GenUpdateArgs(C.Structure):
     _fields_ = [("stage", I32), ("pad", I32), ("dt_factor", C.c_double), ("a", C.c_double), ("b", C.c_double)] + [
         (n, P) for n in ("V", "U0", "F", "wave", "dt", "out", "partial")]
@@ -262,6 +269,8 @@ SIGNATURES = [
     ("nzb_gen_limit", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), P, P, P]),
     ("nzb_gen_update", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.POINTER(GenUpdateArgs), P]),
     ("nzb_gen_blocks", I64, [C.POINTER(GenMesh)]),
+    ("nzb_gen_geometry", C.c_int, [C.POINTER(GenMesh), C.POINTER(GenGeometryArgs), P]),
+    ("nzb_gen_superbee", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), P, P, P, P, P, P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

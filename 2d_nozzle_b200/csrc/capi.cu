@@ -750,6 +750,35 @@ static int check_gen(const nzb_gen_mesh* m, const nzb_physics* ph) {
 
 int64_t nzb_gen_blocks(const nzb_gen_mesh* mesh) { return mesh ? (mesh->n_elem + 127) / 128 : -1; }
 
+int nzb_gen_superbee(const nzb_gen_mesh* mesh, const nzb_physics* phys, double* U, const double* share,
+                     double* means, double* scale, unsigned long long* counters, void* stream) {
+  if (check_gen(mesh, phys)) return -1;
+  if (!U || !share || !means || !scale) return fail("gen_superbee: null array");
+  if (!mesh->mean_weights) return fail("gen_superbee: the mesh lacks mean_weights");
+  return cuda_check(gen_superbee_launch(*mesh, *phys, U, share, means, scale, counters, (cudaStream_t)stream),
+                    "generic superbee launch");
+}
+
+int nzb_gen_geometry(const nzb_gen_mesh* mesh, const nzb_gen_geometry_args* args, void* stream) {
+  if (!mesh || !args) return fail("gen_geometry: null mesh or arguments");
+  const nzb_gen_mesh& m = *mesh;
+  const nzb_gen_geometry_args& a = *args;
+  if (m.np < 1 || m.np > 36 || m.nqv < 1 || m.nqv > 64 || m.nqf < 1 || m.nqf > 16 || (m.nface != 3 && m.nface != 4))
+    return fail("gen_geometry: sizes out of range (NP 1..36, NQV 1..64, NQF 1..16, 3 or 4 faces)");
+  if (a.ng < 3 || a.ng > 16) return fail("gen_geometry: geometry nodes per element out of range (3..16)");
+  if (m.n_elem < 1 || m.n_elem > 0x7fffffff || m.n_int < 0 || m.n_bnd < 0 ||
+      (m.n_int + m.n_bnd + 127) / 128 > 0x7fffffff)
+    return fail("gen_geometry: bad element or edge count");
+  if (!m.phi_vol || !m.phi_face || !m.w_face || !m.face_side || !m.edge_elem || !m.edge_face)
+    return fail("gen_geometry: missing mesh array");
+  if (!a.X || !a.elem_nodes || !a.w_vol || !a.dphi_dxi || !a.dphi_deta || !a.dgeom_dxi || !a.dgeom_deta ||
+      !a.dgeom_dsigma || !a.grad_x || !a.grad_y || !a.grad_x_m || !a.grad_y_m || !a.face_basis_m || !a.inv_mass ||
+      !a.elem_area || !a.mean_weights || !a.edge_normal || !a.edge_jac || !a.edge_length || !a.bad)
+    return fail("gen_geometry: missing argument array");
+  if (cuda_check(cudaMemsetAsync(a.bad, 0, sizeof(int32_t), (cudaStream_t)stream), "gen_geometry memset")) return -1;
+  return cuda_check(gen_geometry_launch(m, a, (cudaStream_t)stream), "gen_geometry launch");
+}
+
 int nzb_gen_rate(const nzb_gen_mesh* mesh, const nzb_physics* phys, int unfolded, const double* U, double* out,
                  double* wave, double* fw, double* smax, void* stream) {
   if (check_gen(mesh, phys)) return -1;

@@ -31,6 +31,10 @@ NZB_INTERNAL cudaError_t gen_limit_launch(const nzb_gen_mesh& m, const nzb_physi
                                           unsigned long long* counters, cudaStream_t st);
 NZB_INTERNAL cudaError_t gen_update_launch(const nzb_gen_mesh& m, const nzb_physics& ph, const nzb_gen_update_args& a,
                                            cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_superbee_launch(const nzb_gen_mesh& m, const nzb_physics& ph, double* U,
+                                             const double* share, double* means, double* scale,
+                                             unsigned long long* counters, cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_geometry_launch(const nzb_gen_mesh& m, const nzb_gen_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t initial_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,
                                             cudaStream_t st);
 NZB_INTERNAL cudaError_t initial_launch_quad(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,

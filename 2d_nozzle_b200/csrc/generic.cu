@@ -1,6 +1,7 @@
 // generic.cu -- launchers of the any-order / curved-element kernels (generic.cuh),
 // instantiated per basis-size bucket.
 #include "forward_dispatch.cuh"
+#include "gen_geometry.cuh"
 #include "generic.cuh"
 
 namespace nzb {
@@ -46,6 +47,33 @@ cudaError_t gen_update_launch(const nzb_gen_mesh& m, const nzb_physics& ph, cons
                               cudaStream_t st) {
   k_gen_update<<<blocks(m.n_elem), 128, 0, st>>>(m, ph, a.stage, a.dt_factor, a.a, a.b, a.V, a.U0, a.F, a.wave, a.dt,
                                                   a.out, a.partial);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_superbee_launch(const nzb_gen_mesh& m, const nzb_physics& ph, double* U, const double* share,
+                                double* means, double* scale, unsigned long long* counters, cudaStream_t st) {
+  k_gen_cell_means<<<blocks(m.n_elem), 128, 0, st>>>(m, U, means);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_gen_lim_scale<<<1, 1024, 0, st>>>(means, m.n_elem, scale);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return by_bucket(m.np, [&](auto B) {
+    k_gen_superbee<decltype(B)::value><<<blocks(m.n_elem), 128, 0, st>>>(m, ph, U, means, scale, share, counters);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t gen_geometry_launch(const nzb_gen_mesh& m, const nzb_gen_geometry_args& a, cudaStream_t st) {
+  const int bytes = GenGeoSmem{m.np, m.nqv, a.ng}.total() * (int)sizeof(double);
+  if (bytes > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_gen_elem_geometry, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  k_gen_elem_geometry<<<(unsigned)m.n_elem, 128, bytes, st>>>(m, a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (m.n_int + m.n_bnd > 0) k_gen_edge_geometry<<<blocks(m.n_int + m.n_bnd), 128, 0, st>>>(m, a);
   return cudaGetLastError();
 }
 

@@ -36,6 +36,7 @@
 
 #include "element.cuh"
 #include "physics.cuh"
+#include "slope.cuh"
 
 namespace nzb {
 
@@ -187,87 +188,81 @@ __device__ void gen_probe_minima(const nzb_gen_mesh& m, const double* Ue, const 
   pmin = pm;
 }
 
-// The positivity limiter in place (src/backends/_numba_kernels.py:927-1093; src/spatial/limiter.py:
-// 103-243): elements it leaves alone are not rewritten.
+// The positivity limiter of one element in place (src/backends/_numba_kernels.py:927-1093;
+// src/spatial/limiter.py:103-243): an element it leaves alone is not rewritten.
 template <int NPB>
-__global__ void __launch_bounds__(128) k_gen_limit(const nzb_gen_mesh m, const nzb_physics ph, double* __restrict__ U,
-                                                   unsigned long long* counters) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int scaled = 0, repaired = 0;
-  if (e < m.n_elem) {
-    const int np = m.np, nf = m.nface;
-    const double g = ph.gamma, g1 = g - 1.0, lam = ph.lebesgue;
-    double* Ue = U + e * np * 4;
-    double ub[4] = {0.0, 0.0, 0.0, 0.0};
+__device__ __forceinline__ void gen_limit_element(const nzb_gen_mesh& m, const nzb_physics& ph, int64_t e,
+                                                  double* __restrict__ Ue, int& scaled, int& repaired) {
+  const int np = m.np, nf = m.nface;
+  const double g = ph.gamma, g1 = g - 1.0, lam = ph.lebesgue;
+  double ub[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int i = 0; i < NPB; ++i) {
-      if (i < np) {
-        const double w = m.mean_weights[e * np + i];
+  for (int i = 0; i < NPB; ++i) {
+    if (i < np) {
+      const double w = m.mean_weights[e * np + i];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) ub[s] = fma(w, Ue[i * 4 + s], ub[s]);
-      }
-    }
-    const double rho_new = ub[0] > ph.rho_floor ? ub[0] : ph.rho_floor;
-    const double e_min = ph.p_floor / g1 + 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / rho_new;
-    const double rhoE_new = ub[3] > e_min ? ub[3] : e_min;
-    const double d0 = rho_new - ub[0], d3 = rhoE_new - ub[3];
-    if (d0 != 0.0 || d3 != 0.0) {
-      for (int i = 0; i < np; ++i) {
-        Ue[i * 4] += d0;
-        Ue[i * 4 + 3] += d3;
-      }
-      ub[0] = rho_new;
-      ub[3] = rhoE_new;
-      repaired = 1;
-    }
-    const double pbar = g1 * (ub[3] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / ub[0]);
-    double eps_r = ph.lim_fraction * ub[0], eps_p = ph.lim_fraction * pbar;
-    eps_r = eps_r < 0.5 * ph.rho_floor ? 0.5 * ph.rho_floor : eps_r;
-    eps_p = eps_p < 0.5 * ph.p_floor ? 0.5 * ph.p_floor : eps_p;
-    double dv[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = 0; i < np; ++i)
-#pragma unroll
-      for (int s = 0; s < 4; ++s) dv[s] = fmax(dv[s], fabs(Ue[i * 4 + s] - ub[s]));
-    bool screened = false;
-    const double rho_lo = ub[0] - lam * dv[0];
-    if (rho_lo >= eps_r) {
-      const double m_hi = sqrt(ub[1] * ub[1] + ub[2] * ub[2]) + lam * sqrt(dv[1] * dv[1] + dv[2] * dv[2]);
-      screened = g1 * (ub[3] - lam * dv[3] - 0.5 * m_hi * m_hi / rho_lo) >= eps_p;
-    }
-    if (!screened) {
-      int fside[8];
-      for (int f = 0; f < nf; ++f) fside[f] = m.face_side[e * nf + f];
-      double rmin, pmin;
-      gen_probe_minima<NPB>(m, Ue, ub, 1.0, fside, g, rmin, pmin);
-      if (rmin < eps_r || pmin < eps_p) {
-        double theta = 1.0;
-        if (rmin < eps_r) {
-          const double gap = ub[0] - rmin;
-          theta = gap <= 0.0 ? 0.0 : (ub[0] - eps_r) / gap;
-          theta = theta < 0.0 ? 0.0 : (theta > 1.0 ? 1.0 : theta);
-        }
-        double rr, ph_;
-        gen_probe_minima<NPB>(m, Ue, ub, theta, fside, g, rr, ph_);
-        if (ph_ < eps_p) {
-          double lo = 0.0, hi = theta;
-          for (int it = 0; it < ph.lim_steps; ++it) {
-            const double mid = 0.5 * (lo + hi);
-            double pm;
-            gen_probe_minima<NPB>(m, Ue, ub, mid, fside, g, rr, pm);
-            if (pm >= eps_p)
-              lo = mid;
-            else
-              hi = mid;
-          }
-          theta = lo;
-        }
-        for (int i = 0; i < np; ++i)
-#pragma unroll
-          for (int s = 0; s < 4; ++s) Ue[i * 4 + s] = ub[s] + theta * (Ue[i * 4 + s] - ub[s]);
-        scaled = 1;
-      }
+      for (int s = 0; s < 4; ++s) ub[s] = fma(w, Ue[i * 4 + s], ub[s]);
     }
   }
+  const double rho_new = ub[0] > ph.rho_floor ? ub[0] : ph.rho_floor;
+  const double e_min = ph.p_floor / g1 + 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / rho_new;
+  const double rhoE_new = ub[3] > e_min ? ub[3] : e_min;
+  const double d0 = rho_new - ub[0], d3 = rhoE_new - ub[3];
+  if (d0 != 0.0 || d3 != 0.0) {
+    for (int i = 0; i < np; ++i) {
+      Ue[i * 4] += d0;
+      Ue[i * 4 + 3] += d3;
+    }
+    ub[0] = rho_new;
+    ub[3] = rhoE_new;
+    repaired = 1;
+  }
+  const double pbar = g1 * (ub[3] - 0.5 * (ub[1] * ub[1] + ub[2] * ub[2]) / ub[0]);
+  double eps_r = ph.lim_fraction * ub[0], eps_p = ph.lim_fraction * pbar;
+  eps_r = eps_r < 0.5 * ph.rho_floor ? 0.5 * ph.rho_floor : eps_r;
+  eps_p = eps_p < 0.5 * ph.p_floor ? 0.5 * ph.p_floor : eps_p;
+  double dv[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = 0; i < np; ++i)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) dv[s] = fmax(dv[s], fabs(Ue[i * 4 + s] - ub[s]));
+  const double rho_lo = ub[0] - lam * dv[0];
+  if (rho_lo >= eps_r) {
+    const double m_hi = sqrt(ub[1] * ub[1] + ub[2] * ub[2]) + lam * sqrt(dv[1] * dv[1] + dv[2] * dv[2]);
+    if (g1 * (ub[3] - lam * dv[3] - 0.5 * m_hi * m_hi / rho_lo) >= eps_p) return;
+  }
+  int fside[8];
+  for (int f = 0; f < nf; ++f) fside[f] = m.face_side[e * nf + f];
+  double rmin, pmin;
+  gen_probe_minima<NPB>(m, Ue, ub, 1.0, fside, g, rmin, pmin);
+  if (!(rmin < eps_r) && !(pmin < eps_p)) return;
+  double theta = 1.0;
+  if (rmin < eps_r) {
+    const double gap = ub[0] - rmin;
+    theta = gap <= 0.0 ? 0.0 : (ub[0] - eps_r) / gap;
+    theta = theta < 0.0 ? 0.0 : (theta > 1.0 ? 1.0 : theta);
+  }
+  double rr, ph_;
+  gen_probe_minima<NPB>(m, Ue, ub, theta, fside, g, rr, ph_);
+  if (ph_ < eps_p) {
+    double lo = 0.0, hi = theta;
+    for (int it = 0; it < ph.lim_steps; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      double pm;
+      gen_probe_minima<NPB>(m, Ue, ub, mid, fside, g, rr, pm);
+      if (pm >= eps_p)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    theta = lo;
+  }
+  for (int i = 0; i < np; ++i)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) Ue[i * 4 + s] = ub[s] + theta * (Ue[i * 4 + s] - ub[s]);
+  scaled = 1;
+}
+
+__device__ __forceinline__ void gen_count(unsigned long long* counters, int scaled, int repaired) {
   if (counters) {
     const int ns = __syncthreads_count(scaled), nr = __syncthreads_count(repaired);
     if (threadIdx.x == 0) {
@@ -275,6 +270,126 @@ __global__ void __launch_bounds__(128) k_gen_limit(const nzb_gen_mesh m, const n
       if (nr) atomicAdd(counters + 1, (unsigned long long)nr);
     }
   }
+}
+
+// The positivity limiter in place, one thread per element.
+template <int NPB>
+__global__ void __launch_bounds__(128) k_gen_limit(const nzb_gen_mesh m, const nzb_physics ph, double* __restrict__ U,
+                                                   unsigned long long* counters) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int scaled = 0, repaired = 0;
+  if (e < m.n_elem) gen_limit_element<NPB>(m, ph, e, U + e * m.np * 4, scaled, repaired);
+  gen_count(counters, scaled, repaired);
+}
+
+// The Superbee TVB slope limiter (src/spatial/limiter.py:246-429) on the generic path, in the
+// specialised kernels' three passes (slope.cuh): the cell averages ubar (E, 4); their maxima
+// max_e |ubar_s| (one block; exact in any order); then per element the factor theta = the
+// minimum over interior faces and components of clip(superbee(a, d) / d, 0, 1), with d the
+// face-averaged own trace minus ubar and a the jump of cell averages across the face, a face
+// quiet where |d| <= 1e-12 or |d| <= tvb (A_e / A_domain) max|ubar_s|; U <- ubar + theta (U -
+// ubar); then the positivity limiter, as apply_limiter runs them.  An element counts as scaled
+// when either limiter changed it.
+__global__ void __launch_bounds__(128) k_gen_cell_means(const nzb_gen_mesh m, const double* __restrict__ U,
+                                                        double* __restrict__ means) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.n_elem) return;
+  const int np = m.np;
+  double ub[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = 0; i < np; ++i) {
+    const double w = m.mean_weights[e * np + i];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) ub[s] = fma(w, U[(e * np + i) * 4 + s], ub[s]);
+  }
+#pragma unroll
+  for (int s = 0; s < 4; ++s) means[e * 4 + s] = ub[s];
+}
+
+__global__ void __launch_bounds__(1024) k_gen_lim_scale(const double* __restrict__ means, int64_t E,
+                                                        double* __restrict__ scale) {
+  __shared__ double red[4][32];
+  double mx[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t e = threadIdx.x; e < E; e += blockDim.x)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) mx[s] = fmax(mx[s], fabs(means[e * 4 + s]));
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    double v = mx[s];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[s][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v = fmax(v, red[threadIdx.x][k]);
+    scale[threadIdx.x] = v;
+  }
+}
+
+template <int NPB>
+__global__ void __launch_bounds__(128) k_gen_superbee(const nzb_gen_mesh m, const nzb_physics ph,
+                                                      double* __restrict__ U, const double* __restrict__ means,
+                                                      const double* __restrict__ scale,
+                                                      const double* __restrict__ share,
+                                                      unsigned long long* counters) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int scaled = 0, repaired = 0;
+  if (e < m.n_elem) {
+    const int np = m.np, nf = m.nface, nqf = m.nqf;
+    double* Ue = U + e * np * 4;
+    double ub[4], sc[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      ub[s] = means[e * 4 + s];
+      sc[s] = scale[s];
+    }
+    const double sh = share[e];
+    double wsum = 0.0;
+    for (int q = 0; q < nqf; ++q) wsum += m.w_face[q];
+    double theta = 1.0;
+    for (int f = 0; f < nf; ++f) {
+      const int64_t k = m.face_edge[e * nf + f];
+      if (k >= m.n_int) continue;  // a boundary face is not limited against
+      const int64_t a0 = m.edge_elem[2 * k], a1 = m.edge_elem[2 * k + 1];
+      const int64_t nb = a0 == e ? a1 : a0;
+      const int side = m.face_side[e * nf + f];
+      const double* pf = m.phi_face + (int64_t)(side * nf + f) * np * nqf;
+      double tm[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int q = 0; q < nqf; ++q) {
+        double tr[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = 0; i < np; ++i) {
+          const double c = pf[i * nqf + q];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) tr[s] = fma(c, Ue[i * 4 + s], tr[s]);
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) tm[s] = fma(m.w_face[q], tr[s], tm[s]);
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const double d = tm[s] / wsum - ub[s];
+        const double a = means[nb * 4 + s] - ub[s];
+        const bool quiet = fabs(d) <= 1e-12 || fabs(d) <= ph.tvb_constant * sh * sc[s];
+        if (!quiet) {
+          double tf = superbee2(a, d) / d;
+          tf = tf < 0.0 ? 0.0 : (tf > 1.0 ? 1.0 : tf);
+          theta = tf < theta ? tf : theta;
+        }
+      }
+    }
+    bool changed = false;
+    for (int i = 0; i < np; ++i)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const double v = ub[s] + theta * (Ue[i * 4 + s] - ub[s]);
+        changed |= v != Ue[i * 4 + s];
+        Ue[i * 4 + s] = v;
+      }
+    gen_limit_element<NPB>(m, ph, e, Ue, scaled, repaired);
+    scaled |= changed ? 1 : 0;
+  }
+  gen_count(counters, scaled, repaired);
 }
 
 // One stage's update per element: stage 1 forms the local step dt = c 2 A / max(wave, FLOOR) and the

@@ -10,9 +10,18 @@ the local step and the weighted norm -- the reference's compiled step
 (src/backends/numba_backend.py:283-337) on the GPU.  The interface is the
 reference's ``Backend`` (src/backends/base.py:81-201), as ``B200Backend``'s.
 
-Not here: the Superbee limiter (its trace averages are built for the
-specialised kernels' tables), the device observables, the device initial
-state and the adjoint, which take straight elements of order 0..3.
+With ``device_metrics=True`` (or lean operators) the coordinate-dependent
+operators are built on the device from the node coordinates instead
+(``nzb_gen_geometry``, csrc/gen_geometry.cuh): the curved (Q = 2) metric terms
+at every volume and face point, the inverse mass matrices and the folded
+operators.
+
+The limiter is the positivity limiter (``nzb_gen_limit``) or the Superbee
+slope limiter followed by it (``nzb_gen_superbee``), as the reference's
+``apply_limiter`` runs them.
+
+Not here: the device observables, the device initial state and the adjoint,
+which take straight elements of order 0..3.
 """
 
 from __future__ import annotations
@@ -37,21 +46,23 @@ def needs_generic(ops) -> bool:
 class GenericB200Backend(B200Backend):
     name = "b200"
 
-    def __init__(self, ops, flow, opts, *, device=None, variants: str = "auto", **_):
+    def __init__(self, ops, flow, opts, *, device=None, variants: str = "auto", device_metrics: bool = False, **_):
+        """``device_metrics``: build the coordinate-dependent operators (gradients, inverse mass, folded
+        operators, edge normals and Jacobians, areas, mean weights) on the device from the node
+        coordinates (``nzb_gen_geometry``) instead of uploading the host's; ``ops`` may then be lean."""
         import torch
 
         self.torch = torch
         self.ops, self.flow, self.opts = ops, flow, opts
         if opts.limiter not in ("positivity", "superbee", "none"):
             raise ValueError(f"unknown limiter {opts.limiter!r}")
-        if opts.limiter == "superbee":
-            raise NotImplementedError("the Superbee limiter runs on straight elements of order 0..3 only")
         self.scheme = recommended_scheme(ops.ref.order) if opts.scheme is None else opts.scheme
         if self.scheme not in SCHEMES:
             raise ValueError(f"unknown scheme {self.scheme!r}; choose from {SCHEMES}")
-        if getattr(ops, "grad_x", None) is None or getattr(ops, "face_basis_m", None) is None:
-            raise ValueError("orders above 3 and curved elements need the full operators "
-                             "(build_operators(..., lean=False))")
+        # lean operators (no per-element gradients) get theirs built on the device
+        device_metrics = bool(device_metrics) or getattr(ops, "grad_x", None) is None \
+            or getattr(ops, "face_basis_m", None) is None
+        self.device_built = bool(device_metrics)
         self.n_limited = 0
         self.n_mean_repaired = 0
         self.n_limit_calls = 0
@@ -72,24 +83,33 @@ class GenericB200Backend(B200Backend):
         f64 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, float)), device=dev)  # noqa: E731
         i32 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a).astype(np.int32)), device=dev)  # noqa: E731
         be, bf = np.asarray(ed.bedge_elem), np.asarray(ed.bedge_face)
+        side = np.asarray(ed.face_side)
         self._arr = {
             "phi_vol": f64(ref.phi_vol), "phi_face": f64(ref.phi_face), "w_face": f64(ref.w_face),
-            "grad_x": f64(ops.grad_x), "grad_y": f64(ops.grad_y), "grad_x_m": f64(ops.grad_x_m),
-            "grad_y_m": f64(ops.grad_y_m), "face_basis_m": f64(ops.face_basis_m), "face_edge": i32(ed.face_edge),
-            "face_side": i32(ed.face_side), "face_sign": f64(ops.face_sign),
+            "face_edge": i32(ed.face_edge), "face_side": i32(side),
+            "face_sign": f64(np.where(side == 0, 1.0, -1.0)),
             "edge_elem": i32(np.concatenate([np.asarray(ed.iedge_elem).reshape(-1, 2), np.stack([be, be], 1)])),
             "edge_face": i32(np.concatenate([np.asarray(ed.iedge_face).reshape(-1, 2), np.stack([bf, bf], 1)])),
             "edge_tag": i32(np.asarray(ed.bedge_tag) if n_bnd else np.zeros(1)),
-            "edge_normal": f64(ops.edge_normal), "edge_jac": f64(ops.edge_jac), "edge_length": f64(ops.edge_length),
-            "elem_area": f64(ops.elem_area), "mean_weights": f64(ops.mean_weights),
         }
+        if device_metrics:
+            self._build_operators(ops, dev, E, NP, NQV, NQF, NF, n_int + n_bnd, f64, i32)
+        else:
+            for k in ("grad_x", "grad_y", "grad_x_m", "grad_y_m", "face_basis_m", "edge_normal", "edge_jac",
+                      "edge_length", "elem_area", "mean_weights"):
+                self._arr[k] = f64(getattr(ops, k))
         m = capi.GenMesh()
         m.np, m.nqv, m.nqf, m.nface = NP, NQV, NQF, NF
         m.n_elem, m.n_int, m.n_bnd = E, n_int, n_bnd
         for k, t in self._arr.items():
-            setattr(m, k, t.data_ptr())
+            if k != "inv_mass":
+                setattr(m, k, t.data_ptr())
         self.gm = m
         self._gm = C.byref(m)
+        if device_metrics:
+            capi.check(self.lib.nzb_gen_geometry(self._gm, C.byref(self._geo_args), self._stream), "nzb_gen_geometry")
+            if int(self._bad.item()):
+                raise ValueError(f"{int(self._bad.item())} quadrature point(s) have a non-positive Jacobian")
         self.phys = physics_struct(flow, opts, ref)
         self._phys_ref = C.byref(self.phys)
         z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
@@ -102,9 +122,55 @@ class GenericB200Backend(B200Backend):
         self._partial = z(self._nb)
         self._res = z(1)
         self._counters = torch.zeros(2, dtype=torch.int64, device=dev)
-        self._minv = None
+        self._minv = self._arr["inv_mass"].view(E, NP, NP) if device_metrics else None
+        if opts.limiter == "superbee":
+            # each element's share of the domain area, as the reference forms it (A_e / sum A)
+            area = self._arr["elem_area"].cpu().numpy()
+            self._share = f64(area / area.sum())
+            self._means, self._scale = z(4 * E), z(4)
         self._obs = None
         self._solvers = {}
+
+    def _build_operators(self, ops, dev, E, NP, NQV, NQF, NF, n_edge, f64, i32):
+        """Output arrays and arguments of nzb_gen_geometry (the coordinate-dependent operators built on
+        the device from the topology's geometry nodes and the node coordinates)."""
+        import torch
+
+        ref, topo = ops.ref, ops.topology
+        X = np.asarray(ops.node_coords, float)
+        en = np.asarray(topo.elem_nodes)
+        NG = int(en.shape[1])
+        if en.shape[0] != E or en.min() < 0 or en.max() >= X.shape[0]:
+            raise ValueError("elem_nodes must index the node coordinates, one row per element")
+        side = np.asarray(topo.edges.face_side)
+        if side.min(initial=0) < 0 or side.max(initial=0) > 1:
+            raise ValueError("face_side must be 0 or 1")
+        shapes = {"dgeom_dxi_vol": (NG, NQV), "dgeom_deta_vol": (NG, NQV), "dphi_dxi_vol": (NP, NQV),
+                  "dphi_deta_vol": (NP, NQV), "w_vol": (NQV,), "dgeom_dsigma_face": (NF, NG, NQF)}
+        for name, shape in shapes.items():
+            if np.asarray(getattr(ref, name)).shape != shape:
+                raise ValueError(f"reference table {name} has shape {np.asarray(getattr(ref, name)).shape}, "
+                                 f"expected {shape}")
+        z = lambda *shape: torch.zeros(shape, dtype=torch.float64, device=dev)  # noqa: E731
+        self._arr.update({
+            "grad_x": z(E, NP, NQV), "grad_y": z(E, NP, NQV), "grad_x_m": z(E, NP, NQV), "grad_y_m": z(E, NP, NQV),
+            "face_basis_m": z(E, NF, NP, NQF), "inv_mass": z(E, NP, NP), "elem_area": z(E), "mean_weights": z(E, NP),
+            "edge_normal": z(n_edge, NQF, 2), "edge_jac": z(n_edge, NQF), "edge_length": z(n_edge),
+        })
+        self._geo_in = {"X": f64(X), "elem_nodes": i32(en), "w_vol": f64(ref.w_vol), "dphi_dxi": f64(ref.dphi_dxi_vol),
+                        "dphi_deta": f64(ref.dphi_deta_vol), "dgeom_dxi": f64(ref.dgeom_dxi_vol),
+                        "dgeom_deta": f64(ref.dgeom_deta_vol), "dgeom_dsigma": f64(ref.dgeom_dsigma_face)}
+        self._bad = torch.zeros(1, dtype=torch.int32, device=dev)
+        a = capi.GenGeometryArgs()
+        a.ng = NG
+        for k, t in self._geo_in.items():
+            setattr(a, k, t.data_ptr())
+        for k in ("grad_x", "grad_y", "grad_x_m", "grad_y_m", "face_basis_m", "inv_mass", "elem_area", "mean_weights",
+                  "edge_normal", "edge_jac", "edge_length"):
+            setattr(a, k, self._arr[k].data_ptr())
+        a.bad = self._bad.data_ptr()
+        self._geo_args = a
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self._geo_in.values())
 
     # -- helpers ----------------------------------------------------------------
     @property
@@ -127,7 +193,13 @@ class GenericB200Backend(B200Backend):
                                          self._stream), "nzb_gen_rate")
 
     def _limit_into(self, t):
-        if self._limiter_on():
+        if not self._limiter_on():
+            return
+        if self.opts.limiter == "superbee" and self.ops.ref.order > 0:
+            capi.check(self.lib.nzb_gen_superbee(self._gm, self._phys_ref, t.data_ptr(), self._share.data_ptr(),
+                                                 self._means.data_ptr(), self._scale.data_ptr(),
+                                                 self._counters.data_ptr(), self._stream), "nzb_gen_superbee")
+        else:
             capi.check(self.lib.nzb_gen_limit(self._gm, self._phys_ref, t.data_ptr(), self._counters.data_ptr(),
                                               self._stream), "nzb_gen_limit")
 

@@ -36,6 +36,8 @@
  *                                                                  src/post/postprocess.py:56-255
  *   nzb_geometry                 the coordinate-dependent part of build_operators
  *                                                                  src/spatial/operators.py:240-303
+ *   nzb_gen_geometry             the same for any order and geometry order, in the
+ *                                 reference's per-element layout   src/spatial/operators.py:209-342
  */
 #ifndef NOZZLE_B200_H
 #define NOZZLE_B200_H
@@ -539,6 +541,51 @@ typedef struct {
 } nzb_gen_update_args;
 int nzb_gen_update(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_update_args* args, void* stream);
 int64_t nzb_gen_blocks(const nzb_gen_mesh* mesh);
+/* The Superbee TVB slope limiter, then the positivity limiter, in place (src/spatial/limiter.py:
+ * 246-429 and apply_limiter): the cell averages into means ((E, 4) scratch), their domain maxima
+ * max_e |ubar_s| into scale (4 scratch), then per element the slope factor from its face-averaged
+ * traces and its neighbours' averages with the threshold tvb share max|ubar_s| (share (E): A_e /
+ * A_domain), and the positivity limiter.  counters (device 2 x uint64, nullable) accumulate the
+ * elements either limiter changed and the repaired ones. */
+int nzb_gen_superbee(const nzb_gen_mesh* mesh, const nzb_physics* phys, double* U, const double* share,
+                     double* means, double* scale, unsigned long long* counters, void* stream);
+
+/* The coordinate-dependent operators of the generic path built on the device
+ * from the node coordinates, for any order and geometry order (the
+ * coordinate part of build_operators, src/spatial/operators.py:209-342): per
+ * element the Jacobian at every volume point, grad_x / grad_y, the mass
+ * matrix and its inverse, grad_x_m / grad_y_m / face_basis_m, the area and the
+ * cell-average weights; per edge (from its owner) the unit normal and
+ * |dX/dsigma| at every face point and the length.  The mesh supplies the
+ * sizes, phi_vol, phi_face, w_face, face_side, edge_elem and edge_face; the
+ * outputs are the arrays a nzb_gen_mesh then points to.  bad (device int32,
+ * zeroed here) counts volume points with a non-positive Jacobian, where the
+ * reference's build raises. */
+typedef struct {
+  int32_t ng;                  /* geometry nodes per element (3 / 4 straight, 6 / 9 curved) */
+  int32_t reserved;
+  const double* X;             /* (n_nodes, 2) node coordinates */
+  const int32_t* elem_nodes;   /* (E, NG) geometry nodes, reference order */
+  const double* w_vol;         /* (NQV) */
+  const double* dphi_dxi;      /* (NP, NQV) */
+  const double* dphi_deta;     /* (NP, NQV) */
+  const double* dgeom_dxi;     /* (NG, NQV) */
+  const double* dgeom_deta;    /* (NG, NQV) */
+  const double* dgeom_dsigma;  /* (NF, NG, NQF) */
+  double* grad_x;              /* (E, NP, NQV) */
+  double* grad_y;
+  double* grad_x_m;
+  double* grad_y_m;
+  double* face_basis_m;        /* (E, NF, NP, NQF) */
+  double* inv_mass;            /* (E, NP, NP) */
+  double* elem_area;           /* (E) */
+  double* mean_weights;        /* (E, NP) */
+  double* edge_normal;         /* (n_edge, NQF, 2) */
+  double* edge_jac;            /* (n_edge, NQF) */
+  double* edge_length;         /* (n_edge) */
+  int32_t* bad;                /* device counter */
+} nzb_gen_geometry_args;
+int nzb_gen_geometry(const nzb_gen_mesh* mesh, const nzb_gen_geometry_args* args, void* stream);
 
 const char* nzb_last_error(void);
 int nzb_version(void);

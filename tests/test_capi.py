@@ -55,7 +55,8 @@ def test_table_sizes_agree_with_the_packer():
 STRUCTS = {"Mesh": "nzb_mesh", "Physics": "nzb_physics", "StageArgs": "nzb_stage_args", "Buffers": "nzb_buffers",
            "BatchMarch": "nzb_batch_march", "AdjointArgs": "nzb_adjoint_args", "AdjointBuffers": "nzb_adjoint_buffers",
            "AdjointMarch": "nzb_adjoint_march", "ObsArgs": "nzb_obs_args", "GeometryArgs": "nzb_geometry_args",
-           "InitialArgs": "nzb_initial_args", "GenMesh": "nzb_gen_mesh", "GenUpdateArgs": "nzb_gen_update_args"}
+           "InitialArgs": "nzb_initial_args", "GenMesh": "nzb_gen_mesh", "GenUpdateArgs": "nzb_gen_update_args",
+           "GenGeometryArgs": "nzb_gen_geometry_args"}
 
 
 def test_struct_layouts_match_the_header(tmp_path):
