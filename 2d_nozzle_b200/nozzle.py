@@ -485,8 +485,11 @@ def quasi1d_table(geom: Geometry, flow) -> np.ndarray:
 
 
 def build_case(*, element="tri", order=1, refine=0, nx=14, nr=5, x_spacing="throat", cluster_strength=3.0,
-               cluster_width=0.12, flow=None, options=None, check_shock=True, lean=False, **geom_kw) -> Case:
-    """A nozzle case with the reference's defaults (src/api.py:159-210).
+               cluster_width=0.12, flow=None, options=None, check_shock=True, lean=False, geometry_order=1,
+               **geom_kw) -> Case:
+    """A nozzle case with the reference's defaults (src/api.py:159-210).  ``geometry_order`` 2 gives
+    curved (quadratic) elements whose interior and mid-edge nodes follow the wall, as the reference's
+    build_nozzle_mesh places them (src/geometry/mesh.py:493-521).
 
     Raises :class:`ShockInNozzle` for an operating point in the shocked band
     unless ``flow.allow_shock_in_nozzle`` -- the reference's refusal
@@ -498,9 +501,11 @@ def build_case(*, element="tri", order=1, refine=0, nx=14, nr=5, x_spacing="thro
     if check_shock and not (is_shock_free(realised_area_ratio(geom), flow.back_pressure_ratio, flow.gamma)
                             or getattr(flow, "allow_shock_in_nozzle", False)):
         raise ShockInNozzle(f"back_pressure_ratio={flow.back_pressure_ratio:.4f} stands a normal shock in the nozzle")
-    topo, _, r_frac = msh.channel_topology(element, nx=nx, nr=nr, refine=refine)
-    x_frac = x_distribution(topo.logical["nx_nodes"], nx, 2**refine, x_spacing, geom.throat_location() / geom.length,
-                            cluster_strength, cluster_width)
+    if geometry_order < 1:
+        raise ValueError(f"geometry_order (Q) must be >= 1, got {geometry_order}")
+    topo, _, r_frac = msh.channel_topology(element, nx=nx, nr=nr, refine=refine, geometry_order=geometry_order)
+    x_frac = x_distribution(topo.logical["nx_nodes"], nx, geometry_order * 2**refine, x_spacing,
+                            geom.throat_location() / geom.length, cluster_strength, cluster_width)
     coords = msh.channel_coords(x_frac, r_frac, geom.wall, geom.length)
     # lean: no per-element operator arrays on the host -- the device builds the metric terms and the
     # initial state from the node coordinates (DeviceMesh.set_geometry, nzb_initial_state)

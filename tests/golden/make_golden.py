@@ -277,6 +277,34 @@ PERF_FIELDS = ("thrust", "thrust_wall", "thrust_imbalance", "thrust_coefficient"
                "ideal_thrust", "thrust_efficiency")
 
 
+def config1_q2():
+    """Config 1 on curved (Q = 2) triangles: the same solve with quadratic geometry (refine 0)."""
+    from src.api import build_case, solve_nozzle
+    from src.post.postprocess import performance
+    from src.timestepping import initialize as ini
+
+    kw = dict(contour="smooth", area_ratio=2.5, element="tri", order=1, refine=0, geometry_order=2, flux="roe",
+              back_pressure_ratio=0.15)
+    cs = build_case(**kw)
+    U0 = ini.initial_state(cs.operators, cs.flow, cs.geometry, "quasi1d")
+    res = solve_nozzle(case=cs, cfl=0.5, tolerance=1e-10, limiter="positivity", scheme="ssprk3", backend="numba",
+                       verbose=False)
+    perf = performance(res)
+    _save(
+        "config1_q2.npz",
+        node_coords=np.asarray(cs.node_coords),
+        elem_nodes=np.asarray(cs.topology.elem_nodes),
+        U0=np.asarray(U0),
+        U_final=np.asarray(res.U),
+        converged=np.bool_(res.converged),
+        iterations=np.int64(res.iterations),
+        residual=np.float64(res.residual),
+        thrust=np.float64(perf.thrust),
+        mass_flow_in=np.float64(perf.mass_flow_in),
+        exit_mach=np.float64(perf.exit_mach_area_averaged),
+    )
+
+
 def observables():
     """The reference's performance() of the tiny cases' states and of config 1's converged state."""
     from types import SimpleNamespace
@@ -613,6 +641,8 @@ if __name__ == "__main__":
         rectangle_microbench()
     if "config1" in which:
         config1()
+    if "config1_q2" in which:
+        config1_q2()
     if "config3" in which:
         config3()
     if "batch" in which:

@@ -8,7 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import pkg, rel, tiny_ops
+from conftest import golden, pkg, rel, tiny_ops
 from oracle import dg_oracle as orc
 from test_oracle_generic import CASES, generic_ops
 
@@ -142,3 +142,24 @@ def test_generic_superbee_follows_the_oracle(cuda, kind, p, q):
     V, res = bk.run(U, 3, "ssprk3")
     W, res_ref = orc.Stepper(ops, flow, opts).run(U.copy(), 3)
     assert rel(V, W) < 1e-11 and abs(res - res_ref) <= 1e-11 * res_ref
+
+
+@pytest.mark.parametrize("device_metrics", [False, True])
+def test_curved_nozzle_solve_matches_the_reference(cuda, device_metrics):
+    """Config 1 on curved (Q = 2) triangles end to end on the generic path: the reference's own
+    solve converges in the same number of iterations to the same thrust, mass flow and exit Mach
+    (1e-10), with the operators uploaded from the host or built on the device."""
+    from test_q2_case import case
+
+    g = golden("config1_q2.npz")
+    full = case()
+    cs = case(lean=device_metrics)
+    bk = pkg("backend").B200Backend(cs.operators, cs.flow, cs.options, device_metrics=device_metrics)
+    assert type(bk).__name__ == "GenericB200Backend" and bk.device_built == device_metrics
+    res = pkg("march").solve(bk, g["U0"], length=cs.geometry.length)
+    assert res.converged, res.message
+    assert res.iterations == int(g["iterations"])
+    perf = pkg("observables").performance(res.U, full.operators, full.flow)
+    for k in ("thrust", "mass_flow_in", "exit_mach"):
+        assert rel(perf[k], g[k]) < 1e-10, k
+    assert rel(res.U, g["U_final"]) < 1e-9
