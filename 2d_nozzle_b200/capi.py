@@ -229,6 +229,12 @@ class GenGeometryArgs(C.Structure):
                          "mean_weights", "edge_normal", "edge_jac", "edge_length", "bad")]
 
 
+class GenInitialArgs(C.Structure):
+    _fields_ = [("ng", I32), ("reserved", I32)] + [
+        (n, P) for n in ("X", "elem_nodes", "geom_vol", "dgeom_dxi", "dgeom_deta", "w_vol", "inv_mass", "wall", "q1d")] + [
+        ("n_q1d", I64), ("out", P)]
+
+
 class GenUpdateArgs(C.Structure):
     _fields_ = [("stage", I32), ("pad", I32), ("dt_factor", C.c_double), ("a", C.c_double), ("b", C.c_double)] + [
         (n, P) for n in ("V", "U0", "F", "wave", "dt", "out", "partial")]
@@ -271,6 +277,7 @@ SIGNATURES = [
     ("nzb_gen_blocks", I64, [C.POINTER(GenMesh)]),
     ("nzb_gen_geometry", C.c_int, [C.POINTER(GenMesh), C.POINTER(GenGeometryArgs), P]),
     ("nzb_gen_superbee", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), P, P, P, P, P, P]),
+    ("nzb_gen_initial_state", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.POINTER(GenInitialArgs), P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

@@ -759,6 +759,21 @@ int nzb_gen_superbee(const nzb_gen_mesh* mesh, const nzb_physics* phys, double* 
                     "generic superbee launch");
 }
 
+int nzb_gen_initial_state(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_initial_args* args,
+                          void* stream) {
+  if (!mesh || !phys || !args) return fail("gen_initial_state: null mesh, physics or arguments");
+  const nzb_gen_mesh& m = *mesh;
+  const nzb_gen_initial_args& a = *args;
+  if (m.np < 1 || m.np > 36 || m.nqv < 1 || m.nqv > 64) return fail("gen_initial_state: sizes out of range");
+  if (a.ng < 3 || a.ng > 16) return fail("gen_initial_state: geometry nodes per element out of range (3..16)");
+  if (m.n_elem < 1 || m.n_elem > 0x7fffffff) return fail("gen_initial_state: bad element count");
+  if (a.n_q1d < 2) return fail("gen_initial_state: the quasi-1D solution needs at least two points");
+  if (!m.phi_vol || !a.X || !a.elem_nodes || !a.geom_vol || !a.dgeom_dxi || !a.dgeom_deta || !a.w_vol ||
+      !a.inv_mass || !a.wall || !a.q1d || !a.out)
+    return fail("gen_initial_state: missing array");
+  return cuda_check(gen_initial_launch(m, *phys, a, (cudaStream_t)stream), "generic initial state launch");
+}
+
 int nzb_gen_geometry(const nzb_gen_mesh* mesh, const nzb_gen_geometry_args* args, void* stream) {
   if (!mesh || !args) return fail("gen_geometry: null mesh or arguments");
   const nzb_gen_mesh& m = *mesh;

@@ -2,6 +2,7 @@
 // instantiated per basis-size bucket.
 #include "forward_dispatch.cuh"
 #include "gen_geometry.cuh"
+#include "gen_initial.cuh"
 #include "generic.cuh"
 
 namespace nzb {
@@ -62,6 +63,13 @@ cudaError_t gen_superbee_launch(const nzb_gen_mesh& m, const nzb_physics& ph, do
     k_gen_superbee<decltype(B)::value><<<blocks(m.n_elem), 128, 0, st>>>(m, ph, U, means, scale, share, counters);
     return cudaGetLastError();
   });
+}
+
+cudaError_t gen_initial_launch(const nzb_gen_mesh& m, const nzb_physics& ph, const nzb_gen_initial_args& a,
+                               cudaStream_t st) {
+  const int bytes = GenInitSmem{m.np, m.nqv, a.ng}.total() * (int)sizeof(double);
+  k_gen_initial_state<<<(unsigned)m.n_elem, 128, bytes, st>>>(m, ph, a);
+  return cudaGetLastError();
 }
 
 cudaError_t gen_geometry_launch(const nzb_gen_mesh& m, const nzb_gen_geometry_args& a, cudaStream_t st) {

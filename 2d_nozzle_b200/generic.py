@@ -20,8 +20,11 @@ The limiter is the positivity limiter (``nzb_gen_limit``) or the Superbee
 slope limiter followed by it (``nzb_gen_superbee``), as the reference's
 ``apply_limiter`` runs them.
 
-Not here: the device observables, the device initial state and the adjoint,
-which take straight elements of order 0..3.
+``initial_state`` projects the quasi-1D state on the device
+(``nzb_gen_initial_state``, csrc/gen_initial.cuh), curved elements included.
+
+Not here: the device observables and the adjoint, which take straight
+elements of order 0..3.
 """
 
 from __future__ import annotations
@@ -254,7 +257,44 @@ class GenericB200Backend(B200Backend):
         return float(((t * w) ** 2).mean().sqrt().item())
 
     def initial_state(self, geometry, host: bool = True):
-        raise NotImplementedError("the device initial state takes straight elements of order 0..3; use the host's")
+        """The quasi-1D initial state of this mesh (src/timestepping/initialize.py:41-102, the reference's
+        ``initial_condition="quasi1d"``) projected on the device (``nzb_gen_initial_state``) from the node
+        coordinates, the nozzle ``geometry`` and this backend's flow: the reference-layout (E, NP, 4) host
+        array, or with ``host=False`` the device tensor of that layout."""
+        from .nozzle import quasi1d_table, wall_parameters
+
+        torch = self.torch
+        ops, ref = self.ops, self.ops.ref
+        dev = self.device
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, float)), device=dev)  # noqa: E731
+        X = np.asarray(ops.node_coords, float)
+        en = np.asarray(ops.topology.elem_nodes)
+        if en.shape[0] != self.E or en.min() < 0 or en.max() >= X.shape[0]:
+            raise ValueError("elem_nodes must index the node coordinates, one row per element")
+        NG, NQV = int(en.shape[1]), int(np.asarray(ref.phi_vol).shape[1])
+        for name in ("geom_vol", "dgeom_dxi_vol", "dgeom_deta_vol"):
+            if np.asarray(getattr(ref, name)).shape != (NG, NQV):
+                raise ValueError(f"reference table {name} does not match the elements' {NG} geometry nodes")
+        if self._minv is None:
+            self._minv = f64(ops.inv_mass)
+        table = quasi1d_table(geometry, self.flow)
+        keep = {"X": f64(X), "elem_nodes": torch.as_tensor(np.ascontiguousarray(en.astype(np.int32)), device=dev),
+                "geom_vol": f64(ref.geom_vol), "dgeom_dxi": f64(ref.dgeom_dxi_vol), "dgeom_deta": f64(ref.dgeom_deta_vol),
+                "w_vol": f64(ref.w_vol), "wall": f64(wall_parameters(geometry)), "q1d": f64(table)}
+        out = torch.empty(self.E * self.NP * 4, dtype=torch.float64, device=dev)
+        a = capi.GenInitialArgs()
+        a.ng = NG
+        for k, t in keep.items():
+            setattr(a, k, t.data_ptr())
+        a.inv_mass = self._minv.data_ptr()
+        a.n_q1d = int(table.shape[1])
+        a.out = out.data_ptr()
+        capi.check(self.lib.nzb_gen_initial_state(self._gm, self._phys_ref, C.byref(a), self._stream),
+                   "nzb_gen_initial_state")
+        if host:
+            return self._get(out)
+        torch.cuda.current_stream(dev).synchronize()  # the inputs above are freed on return
+        return out.view(self.E, self.NP, 4)
 
     def performance(self, U, geom=None) -> dict:
         raise NotImplementedError("the device observables take straight elements of order 0..3")

@@ -38,6 +38,8 @@
  *                                                                  src/spatial/operators.py:240-303
  *   nzb_gen_geometry             the same for any order and geometry order, in the
  *                                 reference's per-element layout   src/spatial/operators.py:209-342
+ *   nzb_initial_state,           initial_state(..., "quasi1d")     src/timestepping/initialize.py:41-102
+ *   nzb_gen_initial_state
  */
 #ifndef NOZZLE_B200_H
 #define NOZZLE_B200_H
@@ -586,6 +588,31 @@ typedef struct {
   int32_t* bad;                /* device counter */
 } nzb_gen_geometry_args;
 int nzb_gen_geometry(const nzb_gen_mesh* mesh, const nzb_gen_geometry_args* args, void* stream);
+
+/* The quasi-1D initial state of one instance on the generic path, projected on
+ * the device (src/timestepping/initialize.py:41-102) as nzb_initial_state does
+ * for the specialised meshes: the point coordinates and Jacobians from the
+ * element's geometry nodes (curved elements included), the wall of
+ * NZB_WALL_PARAMS numbers, the quasi-1D solution, the element's inverse mass;
+ * out is the reference-layout (E, NP, 4) state.  The mesh supplies the sizes
+ * and phi_vol. */
+typedef struct {
+  int32_t ng;                  /* geometry nodes per element */
+  int32_t reserved;
+  const double* X;             /* (n_nodes, 2) */
+  const int32_t* elem_nodes;   /* (E, NG) */
+  const double* geom_vol;      /* (NG, NQV) geometry shape functions at the volume points */
+  const double* dgeom_dxi;     /* (NG, NQV) */
+  const double* dgeom_deta;    /* (NG, NQV) */
+  const double* w_vol;         /* (NQV) */
+  const double* inv_mass;      /* (E, NP, NP) */
+  const double* wall;          /* (NZB_WALL_PARAMS) */
+  const double* q1d;           /* (4, n_q1d): x (increasing), density, axial velocity, pressure */
+  int64_t n_q1d;               /* >= 2 */
+  double* out;                 /* (E, NP, 4) */
+} nzb_gen_initial_args;
+int nzb_gen_initial_state(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_initial_args* args,
+                          void* stream);
 
 const char* nzb_last_error(void);
 int nzb_version(void);
