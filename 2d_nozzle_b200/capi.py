@@ -235,6 +235,12 @@ class GenInitialArgs(C.Structure):
         ("n_q1d", I64), ("out", P)]
 
 
+class GenObsArgs(C.Structure):
+    _fields_ = [("ng", I32), ("reserved", I32)] + [
+        (n, P) for n in ("X", "elem_nodes", "dgeom_dxi", "dgeom_deta", "w_vol", "U")] + [
+        ("s_t", C.c_double), ("r_gas", C.c_double), ("out", P)]
+
+
 class GenUpdateArgs(C.Structure):
     _fields_ = [("stage", I32), ("pad", I32), ("dt_factor", C.c_double), ("a", C.c_double), ("b", C.c_double)] + [
         (n, P) for n in ("V", "U0", "F", "wave", "dt", "out", "partial")]
@@ -278,6 +284,7 @@ SIGNATURES = [
     ("nzb_gen_geometry", C.c_int, [C.POINTER(GenMesh), C.POINTER(GenGeometryArgs), P]),
     ("nzb_gen_superbee", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), P, P, P, P, P, P]),
     ("nzb_gen_initial_state", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.POINTER(GenInitialArgs), P]),
+    ("nzb_gen_observables", C.c_int, [C.POINTER(GenMesh), C.POINTER(Physics), C.POINTER(GenObsArgs), P]),
     ("nzb_limit", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), P, P, P, P]),
     ("nzb_stage", C.c_int, [C.POINTER(Mesh), C.POINTER(Physics), C.POINTER(StageArgs), P]),
     ("nzb_norm_blocks", I64, [I64]),

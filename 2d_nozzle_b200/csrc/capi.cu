@@ -774,6 +774,17 @@ int nzb_gen_initial_state(const nzb_gen_mesh* mesh, const nzb_physics* phys, con
   return cuda_check(gen_initial_launch(m, *phys, a, (cudaStream_t)stream), "generic initial state launch");
 }
 
+int nzb_gen_observables(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_obs_args* args,
+                        void* stream) {
+  if (check_gen(mesh, phys)) return -1;
+  if (!args) return fail("gen_observables: null arguments");
+  const nzb_gen_obs_args& a = *args;
+  if (a.ng < 3 || a.ng > 16) return fail("gen_observables: geometry nodes per element out of range (3..16)");
+  if (!a.X || !a.elem_nodes || !a.dgeom_dxi || !a.dgeom_deta || !a.w_vol || !a.U || !a.out || !mesh->elem_area)
+    return fail("gen_observables: missing array");
+  return cuda_check(gen_observables_launch(*mesh, *phys, a, (cudaStream_t)stream), "generic observables launch");
+}
+
 int nzb_gen_geometry(const nzb_gen_mesh* mesh, const nzb_gen_geometry_args* args, void* stream) {
   if (!mesh || !args) return fail("gen_geometry: null mesh or arguments");
   const nzb_gen_mesh& m = *mesh;

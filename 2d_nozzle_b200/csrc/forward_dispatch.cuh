@@ -36,6 +36,8 @@ NZB_INTERNAL cudaError_t gen_superbee_launch(const nzb_gen_mesh& m, const nzb_ph
                                              unsigned long long* counters, cudaStream_t st);
 NZB_INTERNAL cudaError_t gen_initial_launch(const nzb_gen_mesh& m, const nzb_physics& ph,
                                             const nzb_gen_initial_args& a, cudaStream_t st);
+NZB_INTERNAL cudaError_t gen_observables_launch(const nzb_gen_mesh& m, const nzb_physics& ph,
+                                                const nzb_gen_obs_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t gen_geometry_launch(const nzb_gen_mesh& m, const nzb_gen_geometry_args& a, cudaStream_t st);
 NZB_INTERNAL cudaError_t initial_launch_tri(const nzb_mesh& m, const nzb_physics& ph, const nzb_initial_args& a,
                                             cudaStream_t st);

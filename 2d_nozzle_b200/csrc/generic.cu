@@ -3,6 +3,7 @@
 #include "forward_dispatch.cuh"
 #include "gen_geometry.cuh"
 #include "gen_initial.cuh"
+#include "gen_observe.cuh"
 #include "generic.cuh"
 
 namespace nzb {
@@ -69,6 +70,12 @@ cudaError_t gen_initial_launch(const nzb_gen_mesh& m, const nzb_physics& ph, con
                                cudaStream_t st) {
   const int bytes = GenInitSmem{m.np, m.nqv, a.ng}.total() * (int)sizeof(double);
   k_gen_initial_state<<<(unsigned)m.n_elem, 128, bytes, st>>>(m, ph, a);
+  return cudaGetLastError();
+}
+
+cudaError_t gen_observables_launch(const nzb_gen_mesh& m, const nzb_physics& ph, const nzb_gen_obs_args& a,
+                                   cudaStream_t st) {
+  k_gen_observables<<<1, OBS_BT, 0, st>>>(m, ph, a);
   return cudaGetLastError();
 }
 

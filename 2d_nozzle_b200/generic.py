@@ -23,8 +23,10 @@ slope limiter followed by it (``nzb_gen_superbee``), as the reference's
 ``initial_state`` projects the quasi-1D state on the device
 (``nzb_gen_initial_state``, csrc/gen_initial.cuh), curved elements included.
 
-Not here: the device observables and the adjoint, which take straight
-elements of order 0..3.
+``performance`` integrates the parity observables on the device
+(``nzb_gen_observables``, csrc/gen_observe.cuh).
+
+Not here: batches and the adjoint, which take straight elements of order 0..3.
 """
 
 from __future__ import annotations
@@ -297,7 +299,33 @@ class GenericB200Backend(B200Backend):
         return out.view(self.E, self.NP, 4)
 
     def performance(self, U, geom=None) -> dict:
-        raise NotImplementedError("the device observables take straight elements of order 0..3")
+        """The performance() metrics of a state (src/post/postprocess.py:193-255), integrated on the device
+        (``nzb_gen_observables``); ``geom`` adds the throat-normalised coefficients and the ideal thrust."""
+        from .observables import entropy_reference, from_sums
+
+        torch = self.torch
+        if self._obs is None:
+            ops, ref = self.ops, self.ops.ref
+            dev = self.device
+            f64 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, float)), device=dev)  # noqa: E731
+            en = np.asarray(ops.topology.elem_nodes)
+            X = np.asarray(ops.node_coords, float)
+            if en.shape[0] != self.E or en.min() < 0 or en.max() >= X.shape[0]:
+                raise ValueError("elem_nodes must index the node coordinates, one row per element")
+            self._obs = {"X": f64(X), "elem_nodes": torch.as_tensor(np.ascontiguousarray(en.astype(np.int32)), device=dev),
+                         "dgeom_dxi": f64(ref.dgeom_dxi_vol), "dgeom_deta": f64(ref.dgeom_deta_vol),
+                         "w_vol": f64(ref.w_vol), "out": torch.zeros(capi.NOBS, dtype=torch.float64, device=dev)}
+        src = self._put(U, self._S[0])
+        a = capi.GenObsArgs()
+        a.ng = int(np.asarray(self.ops.topology.elem_nodes).shape[1])
+        for k in ("X", "elem_nodes", "dgeom_dxi", "dgeom_deta", "w_vol", "out"):
+            setattr(a, k, self._obs[k].data_ptr())
+        a.U = src.data_ptr()
+        a.s_t = entropy_reference(self.flow)
+        a.r_gas = float(self.flow.Rgas)
+        capi.check(self.lib.nzb_gen_observables(self._gm, self._phys_ref, C.byref(a), self._stream),
+                   "nzb_gen_observables")
+        return from_sums(self._obs["out"].cpu().numpy(), self.flow, geom)
 
     def step_record(self, U, scheme: str | None = None):
         raise NotImplementedError("stage-by-stage limiter flags come from the specialised kernels")

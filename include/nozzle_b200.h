@@ -40,6 +40,7 @@
  *                                 reference's per-element layout   src/spatial/operators.py:209-342
  *   nzb_initial_state,           initial_state(..., "quasi1d")     src/timestepping/initialize.py:41-102
  *   nzb_gen_initial_state
+ *   nzb_gen_observables          the integrals of performance() on the generic path
  */
 #ifndef NOZZLE_B200_H
 #define NOZZLE_B200_H
@@ -613,6 +614,27 @@ typedef struct {
 } nzb_gen_initial_args;
 int nzb_gen_initial_state(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_initial_args* args,
                           void* stream);
+
+/* The parity observables' NZB_NOBS sums (as nzb_observables) on the generic
+ * path: the boundary integrals with the owner-side traces and the normals and
+ * |dX/dsigma| at every face point, the entropy deviation with w det from the
+ * geometry nodes.  The mesh supplies phi_vol, phi_face, w_face, edge_elem,
+ * edge_face, edge_tag, edge_normal, edge_jac and elem_area. */
+typedef struct {
+  int32_t ng;                  /* geometry nodes per element */
+  int32_t reserved;
+  const double* X;             /* (n_nodes, 2) */
+  const int32_t* elem_nodes;   /* (E, NG) */
+  const double* dgeom_dxi;     /* (NG, NQV) */
+  const double* dgeom_deta;    /* (NG, NQV) */
+  const double* w_vol;         /* (NQV) */
+  const double* U;             /* (E, NP, 4) */
+  double s_t;                  /* the entropy reference p_t^(1 - gamma) (R T_t)^gamma */
+  double r_gas;
+  double* out;                 /* (NZB_NOBS) */
+} nzb_gen_obs_args;
+int nzb_gen_observables(const nzb_gen_mesh* mesh, const nzb_physics* phys, const nzb_gen_obs_args* args,
+                        void* stream);
 
 const char* nzb_last_error(void);
 int nzb_version(void);

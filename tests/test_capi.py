@@ -56,7 +56,8 @@ STRUCTS = {"Mesh": "nzb_mesh", "Physics": "nzb_physics", "StageArgs": "nzb_stage
            "BatchMarch": "nzb_batch_march", "AdjointArgs": "nzb_adjoint_args", "AdjointBuffers": "nzb_adjoint_buffers",
            "AdjointMarch": "nzb_adjoint_march", "ObsArgs": "nzb_obs_args", "GeometryArgs": "nzb_geometry_args",
            "InitialArgs": "nzb_initial_args", "GenMesh": "nzb_gen_mesh", "GenUpdateArgs": "nzb_gen_update_args",
-           "GenGeometryArgs": "nzb_gen_geometry_args", "GenInitialArgs": "nzb_gen_initial_args"}
+           "GenGeometryArgs": "nzb_gen_geometry_args", "GenInitialArgs": "nzb_gen_initial_args",
+           "GenObsArgs": "nzb_gen_obs_args"}
 
 
 def test_struct_layouts_match_the_header(tmp_path):

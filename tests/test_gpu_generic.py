@@ -188,3 +188,32 @@ def test_generic_device_initial_state_matches_the_host(cuda, element, order, q, 
         assert rel(got, want) < (1e-10 if contour.startswith("bezier") else 1e-13), device_metrics
         dev = bk.initial_state(cs.geometry, host=False)
         assert rel(dev.cpu().numpy(), got) == 0.0
+
+
+@pytest.mark.parametrize("kind,p,q", CASES)
+def test_generic_device_observables_match_the_host(cuda, kind, p, q):
+    """nzb_gen_observables against the host integrals (the reference's performance() restated) on every
+    generic fixture mesh, with its operators uploaded or built on the device."""
+    ops, g = generic_ops(kind, p, q)
+    cfg = pkg("config")
+    flow, opts = cfg.FlowConditions(flux="hllc"), cfg.SolverOptions()
+    want = pkg("observables").performance(g["U"], ops, flow)
+    for device_metrics in (False, True):
+        bk = pkg("generic").GenericB200Backend(ops, flow, opts, device_metrics=device_metrics)
+        got = bk.performance(g["U"])
+        for k, v in want.items():
+            assert abs(got[k] - v) <= 1e-11 * max(abs(v), 1e-2), (k, got[k], v)
+
+
+def test_curved_nozzle_observables_are_the_references(cuda):
+    """The device observables of the reference's converged curved-triangle solve against its own
+    performance() (1e-12), with the geometry's throat-normalised coefficients."""
+    from test_q2_case import case
+
+    g = golden("config1_q2.npz")
+    cs = case(lean=True)
+    bk = pkg("backend").B200Backend(cs.operators, cs.flow, cs.options)
+    perf = bk.performance(g["U_final"], cs.geometry)
+    for k in ("thrust", "mass_flow_in", "exit_mach"):
+        assert rel(perf[k], g[k]) < 1e-12, k
+    assert "thrust_coefficient" in perf and np.isfinite(perf["thrust_coefficient"])
