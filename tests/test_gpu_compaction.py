@@ -134,3 +134,27 @@ def test_compacted_batch_gradients_are_the_same(cuda):
         assert (x.adjoint_converged, x.adjoint_iterations) == (y.adjoint_converged, y.adjoint_iterations)
         assert x.value == y.value or (np.isnan(x.value) and np.isnan(y.value))
         assert x.grad == y.grad
+
+
+@pytest.mark.parametrize("variant", ["t1", "split4"])
+def test_an_empty_block_list_launches_nothing(cuda, variant, monkeypatch):
+    """A bucket whose instances have all retired lists no block: the residual leaves every output as it was."""
+    import torch
+
+    monkeypatch.setenv("NZB_VARIANT", variant)
+    capi = pkg("capi")
+    cs = _case(order=3, refine=0)
+    bk = pkg("backend").B200Backend(cs.operators, cs.flow, cs.options)
+    lib, E, NP = bk.lib, bk.mesh.E, bk.mesh.np_
+    src = bk.mesh.pack(cs.initial_state(), torch.empty(4 * NP * E, dtype=torch.float64, device="cuda"))
+    blocks = torch.zeros(1, dtype=torch.int32, device="cuda")
+    mc = capi.Mesh()
+    C.memmove(C.byref(mc), bk.mesh.c_ref, C.sizeof(capi.Mesh))
+    mc.fwd_blocks, mc.n_fwd_blocks = blocks.data_ptr(), 0
+    out = torch.full_like(src, 3.5)
+    wave = torch.full((E,), -1.0, dtype=torch.float64, device="cuda")
+    for op in (0, 1):
+        capi.check(lib.nzb_residual(C.byref(mc), bk._phys_ref, op, src.data_ptr(), out.data_ptr(), wave.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream), "nzb_residual (empty list)")
+    torch.cuda.synchronize()
+    assert bool((out == 3.5).all()) and bool((wave == -1.0).all())
