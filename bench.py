@@ -252,7 +252,7 @@ def microbench(torch, lib_capi, B, cfg, peak_gbs, peak_kind, nx=1000, nr=500, ki
     k = out["kernels"][dom]
     # DRAM bytes per element of each kernel from an ncu capture of 490,000 cubic triangles
     # (profiles/k_element_stage_tri_p3_490k.md), scaled to this launch by its element count
-    traffic = ({"residual_roe": 1055.0, "stage1_hllc": 1135.0, "stage2_hllc": 1503.0, "stage3_hllc": 1447.0}
+    traffic = ({"residual_roe": 1055.0, "stage1_hllc": 1139.0, "stage2_hllc": 1510.0, "stage3_hllc": 1446.0}
                if (kind, order) == ("tri", 3) else {})
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": k["gbs"], "peak": peak_gbs, "unit": "GB/s",
                        "frac": k["gbs"] / peak_gbs, "peak_source": peak_kind,
