@@ -189,6 +189,31 @@ def generic_cases():
         _save(f"tiny_{kind}_p{p}_q{q}.npz", **arrays)
 
 
+def generic_superbee_cases():
+    """The Superbee slope limiter (then positivity) on the generic meshes: the fixture state with per-node
+    jumps of up to 30 % (seed 7) and the TVB constant 0.5, so that most elements are limited; and three
+    SSP-RK3 steps with it."""
+    from src.api import build_case
+    from src.backends import get_backend
+    from src.config import SolverOptions
+    from src.spatial import limiter as lim
+
+    for kind, p, q in GENERIC_CASES:
+        cs = build_case(contour="smooth", element=kind, order=p, refine=0, geometry_order=q)
+        ops = cs.operators
+        U = random_state(ops.n_elem, ops.ref.n_basis)
+        rng = np.random.default_rng(7)
+        U = U * (1.0 + 0.3 * rng.uniform(-1.0, 1.0, size=U.shape[:2])[..., None])
+        arrays = {"U": U,
+                  "superbee": lim.superbee_limiter(U, ops, cs.flow, tvb_constant=0.5),
+                  "superbee_positivity": lim.apply_limiter(U, ops, cs.flow, "superbee", tvb_constant=0.5)}
+        bk = get_backend("numpy", ops, cs.flow, SolverOptions(limiter="superbee", scheme="ssprk3", tvb_constant=0.5))
+        V, res = bk.run(U.copy(), 3, "ssprk3")
+        arrays["run3_ssprk3"] = np.asarray(V)
+        arrays["run3_ssprk3_res"] = np.float64(res)
+        _save(f"tiny_{kind}_p{p}_q{q}_superbee.npz", **arrays)
+
+
 def superbee_cases():
     """The Superbee TVB slope limiter on a rough state of every tiny mesh, and three SSP-RK3 steps with it."""
     from src.api import build_case
@@ -661,3 +686,5 @@ if __name__ == "__main__":
         drop_in_traces()
     if "generic" in which:
         generic_cases()
+    if "generic_superbee" in which:
+        generic_superbee_cases()

@@ -38,3 +38,22 @@ def test_oracle_matches_the_reference(kind, p, q):
     assert rel(L, g["limited_bad"]) < 1e-13
     V, res = orc.Stepper(ops, cfg.FlowConditions(), cfg.SolverOptions(scheme="ssprk3")).run(g["U"].copy(), 3)
     assert rel(V, g["run3_ssprk3"]) < 1e-12 and abs(res - g["run3_ssprk3_res"]) <= 1e-12 * g["run3_ssprk3_res"]
+
+
+@pytest.mark.parametrize("kind,p,q", CASES)
+def test_oracle_superbee_matches_the_reference_on_generic_meshes(kind, p, q):
+    """The oracle's Superbee (then positivity) and three SSP-RK3 steps with it against the reference's own
+    superbee_limiter, apply_limiter and NumPy backend on the generic meshes (tiny_*_superbee.npz: the
+    fixture state with per-node jumps, TVB constant 0.5).  The device's generic Superbee is checked
+    against this oracle on the same states."""
+    ops, _ = generic_ops(kind, p, q)
+    f = golden(f"tiny_{kind}_p{p}_q{q}_superbee.npz")
+    cfg = pkg("config")
+    sb, changed = orc.superbee(f["U"], ops, 0.5)
+    assert changed.sum() > 0
+    assert rel(sb, f["superbee"]) < 1e-13
+    assert rel(orc.positivity(sb, ops, cfg.FlowConditions())[0], f["superbee_positivity"]) < 1e-13
+    W, res = orc.Stepper(ops, cfg.FlowConditions(), cfg.SolverOptions(scheme="ssprk3", limiter="superbee",
+                                                                      tvb_constant=0.5)).run(f["U"].copy(), 3)
+    assert rel(W, f["run3_ssprk3"]) < 1e-12
+    assert abs(res - f["run3_ssprk3_res"]) <= 1e-12 * f["run3_ssprk3_res"]
